@@ -1,0 +1,248 @@
+/*
+ * maomi_b200.h -- C ABI of the B200-native MaoMi optical stage.
+ *
+ * Plain C: device pointers, sizes and a cudaStream_t (passed as void*).  No
+ * entry point allocates device memory; buffers and workspaces belong to the
+ * caller (query sizes with the *_workspace_size functions).  Every entry
+ * point returns MM_OK (0) or a negative status and records a message that
+ * mm_last_error() returns (thread-local).  Kernels run on the given stream
+ * and the calls do not synchronise unless stated.
+ *
+ * Each declaration names the reference interface it replaces (paths relative
+ * to the MaoMi 0.8.0b1 source tree).
+ */
+#ifndef MAOMI_B200_H
+#define MAOMI_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  MM_OK = 0,
+  MM_ERR_ARGUMENT = -1,   /* shape, size or range error (Python: ValueError) */
+  MM_ERR_CUDA = -2,       /* CUDA runtime error (Python: RuntimeError)       */
+  MM_ERR_TIMEOUT = -3,    /* a bounded device wait gave up (RuntimeError)    */
+  MM_ERR_NONFINITE = -4,  /* non-finite input rejected (ValueError)          */
+  MM_ERR_UNSUPPORTED = -5 /* no kernel for this size (ValueError)            */
+};
+
+/* Library version (major*10000 + minor*100 + patch). */
+int mm_version(void);
+
+/* Message of the last failing call on this host thread ("" if none). */
+const char* mm_last_error(void);
+
+/* 1 if the current device is an sm_100 part the library was built for. */
+int mm_device_supported(void);
+
+/* ------------------------------------------------------------------------
+ * Screen gather: dst[b,z,x,y] = src[z, off[b,0]+x, off[b,1]+y] * edge[x*N+y]
+ * Replaces gather_screens, maomi/backends/cuda/optical_kernels.cu:3-12
+ * (bound by gather(), maomi/backends/cuda/native.py:19-24).
+ */
+int mm_gather_screens(const void* src /* float2 (Z,H,W) */, const float* edge /* (N,N) */,
+                      const int32_t* offsets /* (B,2) */, void* dst /* float2 (B,Z,N,N) */,
+                      int B, int Z, int H, int W, int N, void* stream);
+
+/* ------------------------------------------------------------------------
+ * Sparse separable power resample: out[b,x,y,z] = scale*axial[z] *
+ *   sum_i wx[x,i] sum_j wy[y,j] |field[b,z,ix[x,i],iy[y,j]]|^(2*order)
+ * Replaces resample_power, maomi/backends/cuda/optical_kernels.cu:14-38
+ * (bound by ResamplePlan.__call__, maomi/backends/cuda/native.py:68-105).
+ */
+int mm_resample_power(const void* field /* float2 (B,Z,H,W) */, const int32_t* ix, const float* wx,
+                      const int32_t* iy, const float* wy, const float* axial /* (Z) */,
+                      float* out /* (B,X,Y,Z) */, int B, int Z, int H, int W, int X, int Y,
+                      int KX, int KY, int order, float scale, void* stream);
+
+/* ------------------------------------------------------------------------
+ * MATLAB v4 Green-function evaluation in FP64:
+ *   out[q,c] = sum_i g(|query_q - p_i|^2) * coef[i,c],  g(r2) = r2*(0.5*log(r2)-1), g(0)=0
+ * Replaces green_apply, maomi/backends/cuda/interpolation.cu:3-19 (bound by
+ * evaluate_v4, maomi/backends/cuda/interpolation.py:17-38).  Any ncoef >= 1.
+ */
+int mm_green_apply(const double* points /* (n,2) */, const double* coef /* (n,ncoef) */,
+                   const double* queries /* (m,2) */, double* out /* (m,ncoef) */,
+                   int n, int m, int ncoef, void* stream);
+
+/* Dense v4 system matrix G[i,j] = |p_i-p_j|^2 (log|p_i-p_j| - 1), G[i,i] = 0
+ * (the matrix solved in maomi/numerics.py:122-129). */
+int mm_green_matrix(const double* points /* (n,2) */, double* G /* (n,n) */, int n, void* stream);
+
+/* v4 evaluation on a regular pixel grid (queries (i+0.5, j+0.5), i<X, j<Y),
+ * the mask-assembly case of maomi/fixed.py:141-144; out is (X,Y,ncoef). */
+int mm_green_apply_grid(const double* points, const double* coef, double* out,
+                        int n, int X, int Y, int ncoef, void* stream);
+
+/* ------------------------------------------------------------------------
+ * Phase preparation: screens[z,x,y] = exp(1j * resize(raw, ss)[x,y,z] * scale)
+ * with resize = separable index/weight tables (MATLAB imresize bicubic).
+ * Replaces the phase preparation of maomi/backends/cuda/batched.py:52-60
+ * (and optics.py:238-249 with numerics.py:15-39).  raw is (H,W,Z) float32
+ * (XY-major, Z fastest as the reference's arrays); tables are (Ho,KX),(Wo,KY).
+ */
+int mm_phase_prepare(const float* raw, int H, int W, int Z,
+                     const int32_t* ix, const float* wx, int Ho, int KX,
+                     const int32_t* iy, const float* wy, int Wo, int KY,
+                     float scale, void* screens /* float2 (Z,Ho,Wo) */,
+                     float* scratch /* float (Ho,W,Z) when KX>1 or KY>1, else NULL */, void* stream);
+
+/* ------------------------------------------------------------------------
+ * Gaussian pupil with aperture, focusing phase and optional Zernike / custom
+ * phase, evaluated in FP64 and rounded to complex64.
+ * Replaces maomi.optics.pupil, maomi/optics.py:90-117 with
+ * maomi/_optical_math.py:232-296.
+ */
+typedef struct {
+  int n;                 /* grid points per axis                                */
+  double pitch;          /* grid pitch D1 (m)                                    */
+  double beam_radius;    /* Gaussian 1/e radius `rad` (m)                        */
+  double aperture;       /* objective aperture radius `objrad` (m)               */
+  double k;              /* wavenumber 2*pi*n/lambda (1/m)                       */
+  double focal_length;   /* fl (m)                                               */
+  int nmodes;            /* Zernike modes (0 = none)                             */
+  const double* mode_coef;   /* host: per mode, weight*lambda (m) times norm      */
+  const int* mode_m;         /* host: azimuthal order                             */
+  const int* mode_cos;       /* host: 1 = cos(m t), 0 = sin(m t) (m>0)            */
+  const int* mode_nterms;    /* host: radial terms per mode                       */
+  const double* term_coef;   /* host: radial coefficients (concatenated)          */
+  const int* term_pow;       /* host: radial powers (concatenated)                */
+  const float* custom_phase; /* device (Hc,Wc) radians or NULL                    */
+  int custom_h, custom_w;
+  double custom_radius;      /* aperture radius the custom phase spans (m)        */
+  double custom_scale;       /* 1 (radians) or 2*pi (waves)                       */
+} mm_pupil_desc;
+
+int mm_pupil(const mm_pupil_desc* desc, void* out /* float2 (n,n) */,
+             double* scratch /* (n*n + 2*1024) doubles */, void* stream);
+
+/* ------------------------------------------------------------------------
+ * Base field: pupil -> tissue top by the scaled two-plane Fresnel step
+ * (pitch d1 -> d2), then unit L2 norm.  Chirp phases in FP64.
+ * Replaces the base computation of maomi/backends/cuda/batched.py:43-51
+ * (maomi/numerics.py:156-210 with two planes; maomi/optics.py:223-231).
+ */
+typedef struct {
+  int n;
+  double d1, d2;          /* source / destination pitch (m)                       */
+  double dz;              /* propagation distance (m)                             */
+  double lambda_medium;   /* wavelength / n_r (m)                                 */
+  const float* edge1d;    /* device: 1-D edge window (n)                          */
+} mm_base_desc;
+
+int mm_base_field(const mm_base_desc* desc, const void* pupil /* float2 (n,n) */,
+                  void* out /* float2 (n,n) */, void* work /* float2 (n,n) */,
+                  double* scratch /* 1024 doubles */, void* stream);
+
+/* ------------------------------------------------------------------------
+ * Fused per-site split-step propagation (stages A, B, C), screens applied
+ * from the phase volumes at each site's offset, saved planes reduced in the
+ * same pass: focal |E|^(2*order) crops, top/bottom tail images and profiles.
+ * Replaces the hot loop of OpticalPlan.evaluate,
+ * maomi/backends/cuda/batched.py:157-235 (and the per-site loop of
+ * maomi/optics.py:259-340).
+ */
+typedef struct {
+  int size;                /* window of this stage (n for A and C, n2 for B)      */
+  int steps;               /* propagation steps = screens of this stage           */
+  const void* screens;     /* float2 (steps, vol_h, vol_w) phase volume           */
+  int vol_h, vol_w;
+  const float* edge1d;     /* (size) edge window axis                              */
+  const void* kernels;     /* float2 (steps, size): per-step 1-D transfer function
+                              in FFT order with 1/size folded in                   */
+} mm_stage_desc;
+
+typedef struct {
+  mm_stage_desc stage[3];  /* A, B, C                                             */
+  const void* base;        /* float2 (n,n) field entering stage A                 */
+  int n, n2;
+  int order;               /* photon order 1..3                                   */
+  int cut;                 /* first saved plane of stage A (top tail)             */
+  int focal_x0, focal_y0, focal_h, focal_w;  /* focal crop inside the n2 window   */
+  const float* tail_weight[2]; /* per saved plane: trapezoid*axial (top, bottom)   */
+  /* outputs */
+  float* focal;            /* (P, steps_B, focal_h, focal_w) |E|^(2*order)        */
+  float* tail_image[2];    /* per_site: (P,n2,n2); else (slots,n2,n2) running sums */
+  int tail_per_site;
+  double* tail_profile[2]; /* (P, planes) sum over pixels of |E|^(2*order);
+                              zeroed by the call                                  */
+  const int32_t* offsets;  /* (P,2) window offsets on the screen lattice          */
+  int nsites;
+} mm_stage_plan;
+
+enum { MM_SCHEDULE_PERSISTENT = 0, MM_SCHEDULE_BATCHED = 1 };
+
+/* Bytes of workspace mm_propagate_sites needs for `slots` sites in flight. */
+size_t mm_propagate_workspace_size(const mm_stage_plan* plan, int slots, int schedule);
+
+/* Propagate every site of the plan.  schedule: MM_SCHEDULE_PERSISTENT runs one
+ * persistent launch fed by a device work queue (slots sites in flight);
+ * MM_SCHEDULE_BATCHED launches each segment for `slots` sites at a time.
+ * If tail_per_site is 0 the tail images must be zeroed by the caller before
+ * the first call (they accumulate).  Synchronises the stream only to read
+ * the device error flag when check != 0. */
+int mm_propagate_sites(const mm_stage_plan* plan, int schedule, int slots, void* workspace,
+                       size_t workspace_bytes, int check, void* stream);
+
+/* ------------------------------------------------------------------------
+ * Focal PSF finalisation: psf[p,x,y,z] = scale*axial[z] *
+ *   sum_i wx[x,i] sum_j wy[y,j] focal[p,z,ix[x,i],iy[y,j]]
+ * from the focal |E|^(2*order) crops (sparse resample tables as ResamplePlan
+ * builds them), plus per-site energies (FP64 sums) and, when psf_sum and
+ * psf_abs_sum are given, the site sums of psf and |psf| (FP64).  Replaces the
+ * focal ResamplePlan call of maomi/backends/cuda/batched.py:194-200 and the
+ * reductions of maomi/fixed.py:126,153-154.  psf may be NULL (energies only).
+ */
+int mm_focal_finalize(const float* focal /* (P,Z,H,W) */, const int32_t* ix, const float* wx, int KX,
+                      const int32_t* iy, const float* wy, int KY, const float* axial /* (Z) */, float scale,
+                      int P, int Z, int H, int W, int X, int Y,
+                      float* psf /* (P,X,Y,Z) */, double* energies /* (P) */,
+                      double* psf_sum /* (X,Y,Z) */, double* psf_abs_sum /* (X,Y,Z) */, void* stream);
+
+/* Tail image finalisation: out[x,y] = scale * (Rx (sum_s img_s) Ry^T)[x,y]
+ * with dense float32 resample matrices (the convmask mean of
+ * maomi/fixed.py:181 with batched.py:220-223); scratch holds H*W doubles. */
+int mm_tail_finalize(const float* images /* (S,H,W) */, int S, int H, int W,
+                     const float* rx /* (X,H) */, const float* ry /* (Y,W) */, int X, int Y,
+                     double scale, double* out /* (X,Y) */, double* scratch, void* stream);
+
+/* Per-image sparse resample: out[s,x,y] = scale * sum wx*wy*in[s,ix,iy]
+ * (the per-site tail images of batched.py:220-223). */
+int mm_resample_images(const float* in /* (S,H,W) */, int S, int H, int W, const int32_t* ix, const float* wx,
+                       int KX, const int32_t* iy, const float* wy, int KY, int X, int Y, float scale,
+                       float* out /* (S,X,Y) */, void* stream);
+
+/* ------------------------------------------------------------------------
+ * Local-PSF overlap-add render (RANA compact-support operator), FP64.
+ * One call renders the volume through one FullFieldPSF (one depth):
+ *   out[r] += sum over node pairs (i,j) of tile convolution / correlation.
+ * Replaces LocalFFTPlan.__call__, maomi/rana/_fft.py:74-95 (with the plan
+ * construction of :9-49 done on the host).
+ */
+typedef struct {
+  int sx, sy, sz;          /* volume shape (X,Y,Z)                              */
+  int kx, ky, kz;          /* kernel shape                                      */
+  int nodes_x, nodes_y;    /* field nodes                                       */
+  const double* kernels;   /* (nodes_x, nodes_y, kx, ky, kz)                    */
+  const double* wx;        /* (nodes_x, sx) lateral weights                     */
+  const double* wy;        /* (nodes_y, sy)                                     */
+  int detection;           /* 1: weight sources before convolving              */
+  int correlate;           /* 1: flipped kernel (excitation)                   */
+  int plane;               /* 1: 2-D per-plane, output summed over z (scan_slab) */
+} mm_local_desc;
+
+size_t mm_local_render_workspace_size(const mm_local_desc* desc);
+
+int mm_local_render(const mm_local_desc* desc, const double* source /* (sx,sy,sz) */,
+                    const double* zweight /* (sz) or NULL */, double* out /* (sx,sy[,sz]) */,
+                    void* workspace, size_t workspace_bytes, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MAOMI_B200_H */

@@ -1,0 +1,148 @@
+"""ctypes binding of ``libmaomi_b200.so`` (the C ABI in ``include/maomi_b200.h``).
+
+The library is built in-tree (``python -m maomi_b200.build``).  There is no
+fallback: if the library or a CUDA device is missing every entry point raises.
+"""
+
+import ctypes
+from ctypes import POINTER, Structure, c_double, c_float, c_int, c_size_t, c_void_p, c_char_p
+from pathlib import Path
+
+import numpy as np
+
+LIB_PATH = Path(__file__).resolve().parent / "libmaomi_b200.so"
+
+MM_OK, MM_ERR_ARGUMENT, MM_ERR_CUDA, MM_ERR_TIMEOUT, MM_ERR_NONFINITE, MM_ERR_UNSUPPORTED = 0, -1, -2, -3, -4, -5
+MM_SCHEDULE_PERSISTENT, MM_SCHEDULE_BATCHED = 0, 1
+
+c_int_p = POINTER(c_int)
+c_float_p = POINTER(c_float)
+c_double_p = POINTER(c_double)
+
+
+class StageDesc(Structure):
+    _fields_ = [("size", c_int), ("steps", c_int), ("screens", c_void_p), ("vol_h", c_int), ("vol_w", c_int),
+                ("edge1d", c_void_p), ("kernels", c_void_p)]
+
+
+class StagePlan(Structure):
+    _fields_ = [("stage", StageDesc * 3), ("base", c_void_p), ("n", c_int), ("n2", c_int), ("order", c_int),
+                ("cut", c_int), ("focal_x0", c_int), ("focal_y0", c_int), ("focal_h", c_int), ("focal_w", c_int),
+                ("tail_weight", c_void_p * 2), ("focal", c_void_p), ("tail_image", c_void_p * 2),
+                ("tail_per_site", c_int), ("tail_profile", c_void_p * 2), ("offsets", c_void_p), ("nsites", c_int)]
+
+
+class PupilDesc(Structure):
+    _fields_ = [("n", c_int), ("pitch", c_double), ("beam_radius", c_double), ("aperture", c_double),
+                ("k", c_double), ("focal_length", c_double), ("nmodes", c_int), ("mode_coef", c_double_p),
+                ("mode_m", c_int_p), ("mode_cos", c_int_p), ("mode_nterms", c_int_p), ("term_coef", c_double_p),
+                ("term_pow", c_int_p), ("custom_phase", c_void_p), ("custom_h", c_int), ("custom_w", c_int),
+                ("custom_radius", c_double), ("custom_scale", c_double)]
+
+
+class BaseDesc(Structure):
+    _fields_ = [("n", c_int), ("d1", c_double), ("d2", c_double), ("dz", c_double), ("lambda_medium", c_double),
+                ("edge1d", c_void_p)]
+
+
+class LocalDesc(Structure):
+    _fields_ = [("sx", c_int), ("sy", c_int), ("sz", c_int), ("kx", c_int), ("ky", c_int), ("kz", c_int),
+                ("nodes_x", c_int), ("nodes_y", c_int), ("kernels", c_void_p), ("wx", c_void_p), ("wy", c_void_p),
+                ("detection", c_int), ("correlate", c_int), ("plane", c_int)]
+
+
+# name -> (restype, argtypes)
+SIGNATURES = {
+    "mm_version": (c_int, []),
+    "mm_last_error": (c_char_p, []),
+    "mm_device_supported": (c_int, []),
+    "mm_gather_screens": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int, c_int, c_int, c_int, c_void_p]),
+    "mm_resample_power": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int,
+                                  c_int, c_int, c_int, c_int, c_int, c_int, c_int, c_float, c_void_p]),
+    "mm_green_apply": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int, c_int, c_void_p]),
+    "mm_green_matrix": (c_int, [c_void_p, c_void_p, c_int, c_void_p]),
+    "mm_green_apply_grid": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, c_int, c_int, c_void_p]),
+    "mm_phase_prepare": (c_int, [c_void_p, c_int, c_int, c_int, c_void_p, c_void_p, c_int, c_int, c_void_p, c_void_p,
+                                 c_int, c_int, c_float, c_void_p, c_void_p, c_void_p]),
+    "mm_pupil": (c_int, [POINTER(PupilDesc), c_void_p, c_void_p, c_void_p]),
+    "mm_base_field": (c_int, [POINTER(BaseDesc), c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "mm_propagate_workspace_size": (c_size_t, [POINTER(StagePlan), c_int, c_int]),
+    "mm_propagate_sites": (c_int, [POINTER(StagePlan), c_int, c_int, c_void_p, c_size_t, c_int, c_void_p]),
+    "mm_focal_finalize": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_int, c_void_p, c_float,
+                                  c_int, c_int, c_int, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p,
+                                  c_void_p]),
+    "mm_tail_finalize": (c_int, [c_void_p, c_int, c_int, c_int, c_void_p, c_void_p, c_int, c_int, c_double, c_void_p,
+                                 c_void_p, c_void_p]),
+    "mm_resample_images": (c_int, [c_void_p, c_int, c_int, c_int, c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_int,
+                                   c_int, c_int, c_float, c_void_p, c_void_p]),
+    "mm_local_render_workspace_size": (c_size_t, [POINTER(LocalDesc)]),
+    "mm_local_render": (c_int, [POINTER(LocalDesc), c_void_p, c_void_p, c_void_p, c_void_p, c_size_t, c_void_p]),
+}
+
+_lib = None
+
+
+def load():
+    """Load the library once (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise RuntimeError(f"{LIB_PATH.name} is not built; run `python -m maomi_b200.build`")
+        lib = ctypes.CDLL(str(LIB_PATH))
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+    return _lib
+
+
+def exported_symbols():
+    """Names declared in the header that the binding expects."""
+    return list(SIGNATURES)
+
+
+def last_error():
+    msg = load().mm_last_error()
+    return msg.decode() if msg else ""
+
+
+def check(rc, what=""):
+    """Map a C status to the reference's exception types."""
+    if rc == MM_OK:
+        return
+    msg = last_error() or what
+    if rc in (MM_ERR_ARGUMENT, MM_ERR_NONFINITE, MM_ERR_UNSUPPORTED):
+        raise ValueError(msg)
+    raise RuntimeError(msg)
+
+
+def call(name, *args):
+    check(getattr(load(), name)(*args), name)
+
+
+def require_cuda(device):
+    """Product entry points run on CUDA only (no CPU fallback)."""
+    import torch
+    if not str(device).startswith("cuda"):
+        raise ValueError("Use reference optics for CPU")
+    if not torch.cuda.is_available():
+        raise RuntimeError("CUDA-enabled PyTorch and an NVIDIA GPU are required")
+    load()
+
+
+def ptr(t):
+    """Device (or host) address of a tensor / None."""
+    if t is None:
+        return None
+    return c_void_p(t.data_ptr())
+
+
+def stream_of(device=None):
+    import torch
+    return c_void_p(torch.cuda.current_stream(device).cuda_stream)
+
+
+def host_array(values, ctype):
+    a = np.ascontiguousarray(values)
+    return (ctype * max(1, len(a)))(*a.tolist())

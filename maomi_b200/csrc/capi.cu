@@ -1,0 +1,38 @@
+// Library-level entry points: version, error reporting, device check.
+#include <string>
+
+#include "common.cuh"
+
+namespace mm {
+
+namespace {
+thread_local std::string g_error;
+}
+
+void set_error(const char* fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_error = buf;
+}
+
+int cuda_status(cudaError_t e, const char* what) {
+  set_error("%s: %s (%s)", what, cudaGetErrorString(e), cudaGetErrorName(e));
+  return MM_ERR_CUDA;
+}
+
+}  // namespace mm
+
+extern "C" int mm_version(void) { return 100; }
+
+extern "C" const char* mm_last_error(void) { return mm::g_error.c_str(); }
+
+extern "C" int mm_device_supported(void) {
+  int dev = 0, major = 0, minor = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+  if (cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev) != cudaSuccess) return 0;
+  if (cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, dev) != cudaSuccess) return 0;
+  return major == 10 && minor == 0;
+}

@@ -1,0 +1,550 @@
+// Fused split-step propagation of many sites through the A/B/C screen stacks.
+//
+// Each propagation step u <- IDFT2(Q * DFT2(u * S)) has a separable transfer
+// function Q = Qx (x) Qy, so it factors into one 1-D propagate along rows and
+// one along columns.  A "segment" applies, along one axis, the second half of
+// step k-1, the screen of step k, the plane save, and the first half of step
+// k; consecutive segments alternate axes.  The field therefore crosses global
+// memory once per step (read + write) and every line is transformed fully in
+// registers and shared memory.  Saved planes are reduced in the same pass:
+// focal |E|^(2*order) crops, the tail images (trapezoid * axial weighted sums)
+// and the per-plane tail profiles.
+//
+// Two schedules share the segment code:
+//  * persistent: one launch; CTAs pull (site, segment, line-block) items from
+//    a device queue in dependency order and wait (bounded) on per-slot
+//    counters; `slots` sites are in flight, so their fields stay L2-resident.
+//  * batched: one launch per segment for a batch of sites (kernel boundaries
+//    order the segments), the launch structure of the reference's batches.
+#include <algorithm>
+#include <vector>
+
+#include "common.cuh"
+#include "dft.cuh"
+
+namespace mm {
+namespace {
+
+struct StageP {
+  int size, steps, nseg, nblocks;
+  const float2* screens;
+  int vol_h, vol_w;
+  const float* edge;
+  const float2* kern;
+  long long cum0;  // blocks of one site before this stage's first segment
+  int seg0;        // global segment index of this stage's first segment
+};
+
+struct Params {
+  StageP st[3];
+  const float2* base;
+  int n, n2, crop0, order, cut;
+  int fx0, fy0, fh, fw;
+  const float* tail_w[2];
+  float* focal;
+  float* tail_img[2];
+  int tail_per_site;
+  double* profile[2];
+  int planes[2];
+  const int* offsets;
+  int nsites;
+  float2* bufA;
+  float2* bufB;
+  int slots;
+  unsigned* counters;
+  unsigned* head;
+  int* error;
+  long long blocks_per_site;
+  long long total_items;
+  // batched schedule: the stage / segment and first site of this launch
+  int b_stage, b_k, b_site0;
+};
+
+constexpr long long kSpinLimit = 1ll << 24;  // ~ seconds with the backoff below
+
+struct Item {
+  int stage, k, slot, block, site, wave;
+};
+
+__device__ __forceinline__ bool decode(const Params& p, long long item, Item& it) {
+  const long long per_wave = p.blocks_per_site * p.slots;
+  it.wave = int(item / per_wave);
+  long long r = item % per_wave;
+  for (int s = 0; s < 3; ++s) {
+    const long long span = (long long)p.st[s].nseg * p.st[s].nblocks * p.slots;
+    if (r < span || s == 2) {
+      const long long per_seg = (long long)p.st[s].nblocks * p.slots;
+      it.stage = s;
+      it.k = int(r / per_seg);
+      const long long rem = r % per_seg;
+      it.slot = int(rem / p.st[s].nblocks);
+      it.block = int(rem % p.st[s].nblocks);
+      break;
+    }
+    r -= span;
+  }
+  it.site = it.wave * p.slots + it.slot;
+  return it.site < p.nsites;
+}
+
+__device__ __forceinline__ float block_sum(float v, float* red) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  __syncthreads();
+  if (lane == 0) red[warp] = v;
+  __syncthreads();
+  float s = 0.f;
+  if (threadIdx.x == 0)
+    for (int w = 0; w < int(blockDim.x >> 5); ++w) s += red[w];
+  return s;  // valid in thread 0
+}
+
+// Twiddle tables for an N = R1*R2 line, in FP64 rounded once to float.
+template <class L>
+__device__ void fill_twiddles(float2* twf, float2* twi) {
+  for (int i = threadIdx.x; i < L::N; i += blockDim.x) {
+    {  // twf[k1*R2 + t] = exp(-2 pi i t k1 / N)
+      const int k1 = i / L::R2, t = i % L::R2;
+      double s, c;
+      sincospi(-2.0 * double((t * k1) % L::N) / L::N, &s, &c);
+      twf[i] = make_float2(float(c), float(s));
+    }
+    {  // twi[n*R1 + k1] = exp(+2 pi i n k1 / N)
+      const int nn = i / L::R1, k1 = i % L::R1;
+      double s, c;
+      sincospi(2.0 * double((nn * k1) % L::N) / L::N, &s, &c);
+      twi[i] = make_float2(float(c), float(s));
+    }
+  }
+}
+
+// One (site, segment, line block) work item.
+template <class L, int LINES>
+__device__ void process(const Params& p, const Item& it, float2* xa, float2* xb, const float2* twf,
+                        const float2* twi, float* red) {
+  constexpr int R1 = L::R1, R2 = L::R2;
+  const StageP& st = p.st[it.stage];
+  const int N = st.size;
+  const int axis = (st.seg0 + it.k) & 1;  // 0: lines are rows, 1: lines are columns
+  const int tid = threadIdx.x;
+  const int line_local = axis == 0 ? tid / R2 : tid % LINES;
+  const int t = axis == 0 ? tid % R2 : tid / LINES;
+  const int line = it.block * LINES + line_local;
+  float2* xa_l = xa + line_local * L::XBUF;
+  float2* xb_l = xb + line_local * L::XBUF;
+
+  float2 v[R1];
+  // ------------------------------------------------------------------ load
+  {
+    const size_t slot_a = (size_t)it.slot * p.n * p.n;
+    const size_t slot_b = (size_t)it.slot * p.n2 * p.n2;
+#pragma unroll
+    for (int j = 0; j < R1; ++j) {
+      const int e = t + R2 * j;
+      const int row = axis == 0 ? line : e;
+      const int col = axis == 0 ? e : line;
+      float2 a;
+      if (it.k > 0) {
+        const float2* buf = (it.stage == 1) ? p.bufB + slot_b : p.bufA + slot_a;
+        a = __ldcg(buf + (size_t)row * N + col);
+      } else if (it.stage == 0) {
+        a = __ldg(p.base + (size_t)row * N + col);
+      } else if (it.stage == 1) {
+        a = __ldcg(p.bufA + slot_a + (size_t)(row + p.crop0) * p.n + (col + p.crop0));
+      } else {
+        const int r2 = row - p.crop0, c2 = col - p.crop0;
+        a = (r2 >= 0 && r2 < p.n2 && c2 >= 0 && c2 < p.n2)
+                ? __ldcg(p.bufB + slot_b + (size_t)r2 * p.n2 + c2)
+                : make_float2(0.f, 0.f);
+      }
+      v[j] = a;
+    }
+  }
+  // ---------------------------------------- second half of step k-1
+  if (it.k > 0) L::propagate(v, t, st.kern + (size_t)(it.k - 1) * N, xa_l, xb_l, twf, twi);
+  // ------------------------------------------------------- screen of step k
+  if (it.k < st.steps) {
+    const float2* scr = st.screens + (size_t)it.k * st.vol_h * st.vol_w;
+    int xo = __ldg(p.offsets + 2 * it.site), yo = __ldg(p.offsets + 2 * it.site + 1);
+    if (xo < 0 || yo < 0 || xo + N > st.vol_h || yo + N > st.vol_w) {
+      // A window outside the screen volume: flag it (the host reports
+      // MM_ERR_ARGUMENT) and read the volume's corner instead of out of bounds.
+      if (threadIdx.x == 0) atomicOr(p.error, 2);
+      xo = 0;
+      yo = 0;
+    }
+    const float eline = __ldg(st.edge + line);
+#pragma unroll
+    for (int j = 0; j < R1; ++j) {
+      const int e = t + R2 * j;
+      const int row = axis == 0 ? line : e;
+      const int col = axis == 0 ? e : line;
+      const float w = axis == 0 ? eline * __ldg(st.edge + e) : __ldg(st.edge + e) * eline;
+      float2 s = __ldg(scr + (size_t)(xo + row) * st.vol_w + (yo + col));
+      s = make_float2(s.x * w, s.y * w);
+      v[j] = cmul(v[j], s);
+    }
+  }
+  // ------------------------------------------------------------ plane save
+  {
+    int tail = -1, pt = 0;
+    if (it.stage == 0 && it.k >= p.cut) { tail = 0; pt = it.k - p.cut; }
+    if (it.stage == 2) { tail = 1; pt = it.k; }
+    if (tail >= 0) {
+      const float wgt = __ldg(p.tail_w[tail] + pt);
+      float* img = p.tail_img[tail] + (size_t)(p.tail_per_site ? it.site : it.slot) * p.n2 * p.n2;
+      const bool init = p.tail_per_site && pt == 0;
+      float psum = 0.f;
+#pragma unroll
+      for (int j = 0; j < R1; ++j) {
+        const int e = t + R2 * j;
+        const int r2 = (axis == 0 ? line : e) - p.crop0;
+        const int c2 = (axis == 0 ? e : line) - p.crop0;
+        if (r2 >= 0 && r2 < p.n2 && c2 >= 0 && c2 < p.n2) {
+          const float pw = photon_power(v[j], p.order);
+          psum += pw;
+          float* dst = img + (size_t)r2 * p.n2 + c2;
+          const float prev = init ? 0.f : __ldcg(dst);
+          __stcg(dst, prev + wgt * pw);
+        }
+      }
+      const float tot = block_sum(psum, red);
+      if (threadIdx.x == 0) atomicAdd(p.profile[tail] + (size_t)it.site * p.planes[tail] + pt, (double)tot);
+    } else if (it.stage == 1 && it.k < st.steps) {
+      float* dst = p.focal + ((size_t)it.site * st.steps + it.k) * p.fh * p.fw;
+#pragma unroll
+      for (int j = 0; j < R1; ++j) {
+        const int e = t + R2 * j;
+        const int r = (axis == 0 ? line : e) - p.fx0;
+        const int c = (axis == 0 ? e : line) - p.fy0;
+        if (r >= 0 && r < p.fh && c >= 0 && c < p.fw) __stcs(dst + (size_t)r * p.fw + c, photon_power(v[j], p.order));
+      }
+    }
+  }
+  // ---------------------------------------- first half of step k
+  if (it.k < st.steps) L::propagate(v, t, st.kern + (size_t)it.k * N, xa_l, xb_l, twf, twi);
+  // ------------------------------------------------------------------ store
+  if (!(it.stage == 2 && it.k == st.steps)) {
+    float2* buf = (it.stage == 1) ? p.bufB + (size_t)it.slot * p.n2 * p.n2 : p.bufA + (size_t)it.slot * p.n * p.n;
+#pragma unroll
+    for (int j = 0; j < R1; ++j) {
+      const int e = t + R2 * j;
+      const int row = axis == 0 ? line : e;
+      const int col = axis == 0 ? e : line;
+      __stcg(buf + (size_t)row * N + col, v[j]);
+    }
+  }
+}
+
+template <class L, int LINES>
+struct Smem {
+  static constexpr size_t xbuf = (size_t)LINES * L::XBUF;
+  static constexpr size_t bytes = (2 * xbuf + 2 * L::N) * sizeof(float2) + 32 * sizeof(float);
+};
+
+template <class L, int LINES>
+__global__ void __launch_bounds__(LINES * L::R2) persistent_kernel(Params p) {
+  extern __shared__ float4 smem_raw[];
+  float2* xa = reinterpret_cast<float2*>(smem_raw);
+  float2* xb = xa + Smem<L, LINES>::xbuf;
+  float2* twf = xb + Smem<L, LINES>::xbuf;
+  float2* twi = twf + L::N;
+  float* red = reinterpret_cast<float*>(twi + L::N);
+  __shared__ long long s_item;
+  __shared__ int s_abort;
+  fill_twiddles<L>(twf, twi);
+  __syncthreads();
+  while (true) {
+    if (threadIdx.x == 0) s_item = (long long)atomicAdd(p.head, 1u);
+    __syncthreads();
+    const long long item = s_item;
+    if (item >= p.total_items) break;
+    Item it;
+    const bool live = decode(p, item, it);
+    if (live) {
+      if (threadIdx.x == 0) {
+        const StageP& st = p.st[it.stage];
+        const unsigned need = unsigned(it.wave * p.blocks_per_site + st.cum0 + (long long)it.k * st.nblocks);
+        long long spins = 0;
+        unsigned ns = 32;
+        int abort = 0;
+        while (ld_acquire(p.counters + it.slot) < need) {
+          if (++spins > kSpinLimit || (ld_acquire(reinterpret_cast<unsigned*>(p.error)) & 1u) != 0u) {
+            atomicOr(p.error, 1);
+            abort = 1;
+            break;
+          }
+          __nanosleep(ns);
+          ns = ns < 256 ? ns * 2 : 256;
+        }
+        s_abort = abort;
+      }
+      __syncthreads();
+      if (s_abort) break;
+      process<L, LINES>(p, it, xa, xb, twf, twi, red);
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        __threadfence();
+        atomicAdd(p.counters + it.slot, 1u);
+      }
+    }
+    __syncthreads();  // s_item is rewritten next iteration
+  }
+}
+
+template <class L, int LINES>
+__global__ void __launch_bounds__(LINES * L::R2) batched_kernel(Params p) {
+  extern __shared__ float4 smem_raw[];
+  float2* xa = reinterpret_cast<float2*>(smem_raw);
+  float2* xb = xa + Smem<L, LINES>::xbuf;
+  float2* twf = xb + Smem<L, LINES>::xbuf;
+  float2* twi = twf + L::N;
+  float* red = reinterpret_cast<float*>(twi + L::N);
+  fill_twiddles<L>(twf, twi);
+  __syncthreads();
+  const StageP& st = p.st[p.b_stage];
+  Item it;
+  it.stage = p.b_stage;
+  it.k = p.b_k;
+  it.slot = blockIdx.x / st.nblocks;
+  it.block = blockIdx.x % st.nblocks;
+  it.site = p.b_site0 + it.slot;
+  it.wave = 0;
+  if (it.site >= p.nsites) return;
+  process<L, LINES>(p, it, xa, xb, twf, twi, red);
+}
+
+// ------------------------------------------------------------------- host --
+struct Config {
+  int r1, r2, lines;
+};
+
+bool line_config(int n, Config& c) {
+  switch (n) {
+    case 64: c = {8, 8, 32}; return true;
+    case 128: c = {16, 8, 32}; return true;
+    case 256: c = {16, 16, 16}; return true;
+    case 512: c = {32, 16, 8}; return true;
+    default: return false;
+  }
+}
+
+size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+struct Workspace {
+  float2* bufA;
+  float2* bufB;
+  unsigned* counters;
+  unsigned* head;
+  int* error;
+  size_t bytes;
+};
+
+Workspace carve(void* base, int n, int n2, int slots) {
+  Workspace w{};
+  char* p = static_cast<char*>(base);
+  size_t off = 0;
+  auto take = [&](size_t b) {
+    char* q = p ? p + off : nullptr;
+    off += align256(b);
+    return q;
+  };
+  w.bufA = reinterpret_cast<float2*>(take((size_t)slots * n * n * sizeof(float2)));
+  w.bufB = reinterpret_cast<float2*>(take((size_t)slots * n2 * n2 * sizeof(float2)));
+  w.counters = reinterpret_cast<unsigned*>(take((size_t)slots * sizeof(unsigned)));
+  w.head = reinterpret_cast<unsigned*>(take(sizeof(unsigned)));
+  w.error = reinterpret_cast<int*>(take(sizeof(int)));
+  w.bytes = off;
+  return w;
+}
+
+template <class L, int LINES>
+int launch_batched(Params& p, int stage, int k, int site0, int batch, cudaStream_t s) {
+  const size_t smem = Smem<L, LINES>::bytes;
+  MM_CHECK_CUDA(cudaFuncSetAttribute(batched_kernel<L, LINES>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                "cudaFuncSetAttribute(batched)");
+  p.b_stage = stage;
+  p.b_k = k;
+  p.b_site0 = site0;
+  const int grid = batch * p.st[stage].nblocks;
+  batched_kernel<L, LINES><<<grid, LINES * L::R2, smem, s>>>(p);
+  MM_CHECK_LAUNCH("batched propagation kernel");
+  return MM_OK;
+}
+
+int launch_batched_any(Params& p, int stage, int k, int site0, int batch, cudaStream_t s) {
+  switch (p.st[stage].size) {
+    case 64: return launch_batched<FftLine<8, 8>, 32>(p, stage, k, site0, batch, s);
+    case 128: return launch_batched<FftLine<16, 8>, 32>(p, stage, k, site0, batch, s);
+    case 256: return launch_batched<FftLine<16, 16>, 16>(p, stage, k, site0, batch, s);
+    case 512: return launch_batched<FftLine<32, 16>, 8>(p, stage, k, site0, batch, s);
+    default: set_error("no propagation kernel for window %d", p.st[stage].size); return MM_ERR_UNSUPPORTED;
+  }
+}
+
+template <class L, int LINES>
+int launch_persistent(Params& p, cudaStream_t s) {
+  const size_t smem = Smem<L, LINES>::bytes;
+  MM_CHECK_CUDA(cudaFuncSetAttribute(persistent_kernel<L, LINES>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                "cudaFuncSetAttribute(persistent)");
+  int dev = 0, sms = 0, per_sm = 0;
+  MM_CHECK_CUDA(cudaGetDevice(&dev), "cudaGetDevice");
+  MM_CHECK_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "SM count");
+  MM_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, persistent_kernel<L, LINES>, LINES * L::R2, smem),
+                "occupancy");
+  if (per_sm < 1) {
+    set_error("persistent propagation kernel cannot be resident (smem %zu)", smem);
+    return MM_ERR_UNSUPPORTED;
+  }
+  const long long grid = std::min<long long>((long long)sms * per_sm, p.total_items);
+  persistent_kernel<L, LINES><<<(unsigned)grid, LINES * L::R2, smem, s>>>(p);
+  MM_CHECK_LAUNCH("persistent propagation kernel");
+  return MM_OK;
+}
+
+int launch_persistent_any(Params& p, cudaStream_t s) {
+  switch (p.n) {
+    case 64: return launch_persistent<FftLine<8, 8>, 32>(p, s);
+    case 128: return launch_persistent<FftLine<16, 8>, 32>(p, s);
+    case 256: return launch_persistent<FftLine<16, 16>, 16>(p, s);
+    case 512: return launch_persistent<FftLine<32, 16>, 8>(p, s);
+    default: set_error("no propagation kernel for window %d", p.n); return MM_ERR_UNSUPPORTED;
+  }
+}
+
+int build_params(const mm_stage_plan* plan, int slots, Params& p) {
+  MM_CHECK_ARG(plan != nullptr, "plan is NULL");
+  MM_CHECK_ARG(plan->nsites >= 1, "need at least one site (got %d)", plan->nsites);
+  MM_CHECK_ARG(slots >= 1, "slots must be >= 1 (got %d)", slots);
+  MM_CHECK_ARG(plan->order >= 1 && plan->order <= 3, "photon order must be 1, 2 or 3 (got %d)", plan->order);
+  MM_CHECK_ARG(plan->n >= plan->n2 && plan->n2 >= 1 && (plan->n - plan->n2) % 2 == 0,
+               "incompatible windows n=%d n2=%d", plan->n, plan->n2);
+  MM_CHECK_ARG(plan->base && plan->offsets && plan->focal && plan->tail_image[0] && plan->tail_image[1] &&
+                   plan->tail_profile[0] && plan->tail_profile[1] && plan->tail_weight[0] && plan->tail_weight[1],
+               "plan has NULL buffers");
+  p = Params{};
+  long long cum = 0;
+  int seg = 0;
+  for (int s = 0; s < 3; ++s) {
+    const mm_stage_desc& d = plan->stage[s];
+    Config c;
+    MM_CHECK_ARG(d.size == (s == 1 ? plan->n2 : plan->n), "stage %d window %d does not match the plan", s, d.size);
+    if (!line_config(d.size, c)) {
+      set_error("no propagation kernel for window %d (supported: 64, 128, 256, 512)", d.size);
+      return MM_ERR_UNSUPPORTED;
+    }
+    MM_CHECK_ARG(d.steps >= 1 && d.screens && d.edge1d && d.kernels, "stage %d incomplete", s);
+    MM_CHECK_ARG(d.vol_h >= d.size && d.vol_w >= d.size, "stage %d screens smaller than the window", s);
+    StageP& st = p.st[s];
+    st.size = d.size;
+    st.steps = d.steps;
+    st.nseg = d.steps + 1;
+    st.nblocks = d.size / c.lines;
+    st.screens = static_cast<const float2*>(d.screens);
+    st.vol_h = d.vol_h;
+    st.vol_w = d.vol_w;
+    st.edge = d.edge1d;
+    st.kern = static_cast<const float2*>(d.kernels);
+    st.cum0 = cum;
+    st.seg0 = seg;
+    cum += (long long)st.nseg * st.nblocks;
+    seg += st.nseg;
+  }
+  MM_CHECK_ARG(plan->cut >= 0 && plan->cut <= plan->stage[0].steps, "cut %d outside stage A", plan->cut);
+  MM_CHECK_ARG(plan->focal_x0 >= 0 && plan->focal_y0 >= 0 && plan->focal_h >= 1 && plan->focal_w >= 1 &&
+                   plan->focal_x0 + plan->focal_h <= plan->n2 && plan->focal_y0 + plan->focal_w <= plan->n2,
+               "focal crop outside the stage-B window");
+  p.base = static_cast<const float2*>(plan->base);
+  p.n = plan->n;
+  p.n2 = plan->n2;
+  p.crop0 = (plan->n - plan->n2) / 2;
+  p.order = plan->order;
+  p.cut = plan->cut;
+  p.fx0 = plan->focal_x0;
+  p.fy0 = plan->focal_y0;
+  p.fh = plan->focal_h;
+  p.fw = plan->focal_w;
+  p.tail_w[0] = plan->tail_weight[0];
+  p.tail_w[1] = plan->tail_weight[1];
+  p.focal = plan->focal;
+  p.tail_img[0] = plan->tail_image[0];
+  p.tail_img[1] = plan->tail_image[1];
+  p.tail_per_site = plan->tail_per_site;
+  p.profile[0] = plan->tail_profile[0];
+  p.profile[1] = plan->tail_profile[1];
+  p.planes[0] = plan->stage[0].steps + 1 - plan->cut;
+  p.planes[1] = plan->stage[2].steps + 1;
+  p.offsets = plan->offsets;
+  p.nsites = plan->nsites;
+  p.slots = slots;
+  p.blocks_per_site = cum;
+  return MM_OK;
+}
+
+}  // namespace
+}  // namespace mm
+
+extern "C" size_t mm_propagate_workspace_size(const mm_stage_plan* plan, int slots, int schedule) {
+  (void)schedule;
+  if (!plan || slots < 1) return 0;
+  return mm::carve(nullptr, plan->n, plan->n2, slots).bytes;
+}
+
+extern "C" int mm_propagate_sites(const mm_stage_plan* plan, int schedule, int slots, void* workspace,
+                                  size_t workspace_bytes, int check, void* stream) {
+  using namespace mm;
+  Params p;
+  if (int rc = build_params(plan, slots, p)) return rc;
+  MM_CHECK_ARG(schedule == MM_SCHEDULE_PERSISTENT || schedule == MM_SCHEDULE_BATCHED, "unknown schedule %d", schedule);
+  slots = std::min(slots, plan->nsites);
+  if (schedule == MM_SCHEDULE_PERSISTENT) {
+    // Balance the sites over the slots so the last wave is (nearly) full.
+    const int waves = (plan->nsites + slots - 1) / slots;
+    slots = (plan->nsites + waves - 1) / waves;
+  }
+  p.slots = slots;
+  Workspace w = carve(workspace, plan->n, plan->n2, slots);
+  MM_CHECK_ARG(workspace != nullptr && workspace_bytes >= w.bytes,
+               "workspace too small: %zu bytes given, %zu needed", workspace_bytes, w.bytes);
+  MM_CHECK_ARG(reinterpret_cast<uintptr_t>(workspace) % 256 == 0, "workspace must be 256-byte aligned");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  p.bufA = w.bufA;
+  p.bufB = w.bufB;
+  p.counters = w.counters;
+  p.head = w.head;
+  p.error = w.error;
+  for (int t = 0; t < 2; ++t)
+    MM_CHECK_CUDA(cudaMemsetAsync(p.profile[t], 0, sizeof(double) * (size_t)p.planes[t] * plan->nsites, s),
+                  "zero tail profiles");
+  MM_CHECK_CUDA(cudaMemsetAsync(w.counters, 0, (char*)w.error + sizeof(int) - (char*)w.counters, s),
+                "zero queue state");
+  int rc = MM_OK;
+  if (schedule == MM_SCHEDULE_PERSISTENT) {
+    MM_CHECK_ARG(plan->n == plan->n2, "the persistent schedule needs n == n2 (got %d, %d); use the batched one",
+                 plan->n, plan->n2);
+    const int waves = (plan->nsites + slots - 1) / slots;
+    p.total_items = (long long)waves * slots * p.blocks_per_site;
+    rc = launch_persistent_any(p, s);
+  } else {
+    for (int site0 = 0; site0 < plan->nsites && rc == MM_OK; site0 += slots) {
+      const int batch = std::min(slots, plan->nsites - site0);
+      for (int stage = 0; stage < 3 && rc == MM_OK; ++stage)
+        for (int k = 0; k <= p.st[stage].steps && rc == MM_OK; ++k)
+          rc = launch_batched_any(p, stage, k, site0, batch, s);
+    }
+  }
+  if (rc != MM_OK || !check) return rc;
+  MM_CHECK_CUDA(cudaStreamSynchronize(s), "propagation");
+  int err = 0;
+  MM_CHECK_CUDA(cudaMemcpy(&err, w.error, sizeof(int), cudaMemcpyDeviceToHost), "read error flag");
+  if (err & 2) {
+    set_error("a site window lies outside the screen volume (offsets out of range)");
+    return MM_ERR_ARGUMENT;
+  }
+  if (err) {
+    set_error("persistent propagation: a dependency wait timed out");
+    return MM_ERR_TIMEOUT;
+  }
+  return MM_OK;
+}

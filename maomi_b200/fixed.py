@@ -1,0 +1,244 @@
+"""The optical stage on the fixed 65 x 65 site lattice, end to end on the GPU.
+
+Mirrors maomi/fixed.py: ``fixed_locations`` (:15-33), ``field_shapes``
+(:36-56), ``assemble`` (:119-190, the ``matlab_v4`` mode) and ``run_fixed``
+(:193-411).  ``run_stage`` is the fused device path behind them: phase
+preparation, the persistent propagation of every site, both tails reduced on
+the device, focal PSF finalisation with FP64 site sums, and the FP64 v4 mask
+assembly (Green matrix, dense solve and grid evaluation on the GPU).  Only
+the final products are copied to the host.
+"""
+
+import time
+
+import numpy as np
+
+from . import _lib
+from ._optical_math import gaussian_beam_size
+from .numerics import v4_coefficients_device, v4_evaluate_grid_device, v4_interpolate
+
+
+def fixed_locations(config, count_per_axis=65):
+    """Uniform physical XY locations snapped to the supersampled lattice."""
+    if isinstance(count_per_axis, bool) or not isinstance(count_per_axis, int) or count_per_axis < 2:
+        raise ValueError("count_per_axis must be an integer >= 2")
+    ticks = np.asarray(config.volume_um[:2], float) * config.vres * config.ss
+    if (not np.all(np.isfinite(ticks)) or np.any(ticks < count_per_axis - 1)
+            or not np.allclose(ticks, np.round(ticks))):
+        raise ValueError(
+            f"Fixed {count_per_axis}x{count_per_axis} requires an integer optical lattice "
+            f"with at least {count_per_axis} positions per axis; choose count_per_axis explicitly")
+    axes = [np.round(np.linspace(0, int(round(t)), count_per_axis)) / (config.vres * config.ss) for t in ticks]
+    points = np.stack(np.meshgrid(*axes, indexing="ij"), -1).reshape(-1, 2)
+    if len(np.unique(points, axis=0)) != count_per_axis ** 2:
+        raise ValueError("Grid contains duplicate locations")
+    return points
+
+
+def field_shapes(config):
+    """Shapes of the raw A/B/C occupancy fields the stage expects."""
+    v, p = config.parameters()
+    r = config.vres
+    n = int(round((v.vasc_sz[0] - v.vol_sz[0]) * r))
+    n2 = int(round(min(max(gaussian_beam_size(p, config.psf_um[2] / 2, 3)) * r * 2, n))) if config.propcrop else n
+    za = int(round((config.depth_um + config.volume_um[2] / 2 - config.psf_um[2] / 2) * r))
+    zb = int(round(config.psf_um[2] * r))
+    pc = int(round(config.prop_um * r))
+    nc = int(round(config.tail_um * r))
+    if min(za, zb, pc, nc) <= 0:
+        raise ValueError("Optical A/B/C propagation extents must be positive")
+    xy = np.round(np.asarray(config.volume_um[:2]) * r).astype(int)
+    return [(int(xy[0] + n), int(xy[1] + n), int(np.ceil(za / pc))),
+            (int(xy[0] + n2), int(xy[1] + n2), zb),
+            (int(xy[0] + n), int(xy[1] + n), int(np.ceil(nc / pc)))]
+
+
+def _psf_z(config, z, profile):
+    """Tail axial profile resampled to the voxel pitch and normalised to unit mean."""
+    actual = z - z[0]
+    axial = np.arange(round(actual[-1] * 1e6 * config.vres) + 1) / config.vres
+    interp = np.interp(axial, actual * 1e6, profile)
+    return interp / interp.mean() if interp.mean() > 0 else interp
+
+
+def assemble(config, out, shape, *, mask_mode="matlab_v4", z_positions=None, cut=None, device="cuda"):
+    """Masks and averaged PSFs from per-site outputs (fixed.py:119-190).
+
+    Only ``matlab_v4`` is provided (the cubic mode is diagnostic-only in the
+    reference); the v4 system is solved and evaluated on the GPU."""
+    if mask_mode != "matlab_v4":
+        raise ValueError("mask_mode must be matlab_v4 (cubic aggregation is not provided)")
+    points = out["points_um"]
+    psfs = out["psfs"]
+    energies = psfs.sum((1, 2, 3), dtype=np.float64)
+    values = [energies]
+    tails = bool(out["tails_computed"])
+    if tails:
+        values.extend(out[k]["weight"] for k in ("top", "bottom"))
+    values = np.stack(values, axis=1)
+    q = np.stack(np.meshgrid(*[np.arange(k) + 0.5 for k in shape], indexing="ij"), -1)
+    masks = v4_interpolate(points * config.vres, values, q, device=device)
+    mask = masks[..., 0]
+    mean = float(mask.mean())
+    if not np.isfinite(mean) or mean <= 0:
+        raise ValueError("Nonpositive or invalid mean excitation energy")
+    weights = np.full(len(points), 1 / len(points))
+    result = {
+        "psf": (weights @ np.abs(psfs).reshape(len(points), -1)).reshape(psfs.shape[1:]),
+        "psf_raw": (weights @ psfs.reshape(len(points), -1)).reshape(psfs.shape[1:]),
+        "psf_3d": psfs, "points_um": points, "energies": energies,
+        "mask_raw": mask, "mask": mask / mean, "mask_mean": mean, "mask_mode": mask_mode,
+        "geometry_cache_hit": False, "tails_computed": tails, "unique_optical_paths": len(points),
+        "negative_resampling_mass_fraction": float(
+            -np.minimum(psfs, 0).sum(dtype=np.float64) / max(np.abs(psfs).sum(dtype=np.float64), 1e-30)),
+    }
+    if tails:
+        for j, (native, name) in enumerate([("top", "psfT"), ("bottom", "psfB")]):
+            data = out[native]
+            z = z_positions[0][cut:] if j == 0 else z_positions[2]
+            tm = masks[..., j + 1]
+            tm_mean = float(tm.mean())
+            result[name] = {
+                "convmask": data["convmask"].mean(0),
+                "weight": float(data["weight"].mean()),
+                "psfZ": _psf_z(config, z, data["profile"].sum(0, dtype=np.float64)),
+                "mask_raw": tm, "mask": tm / tm_mean if tm_mean > 0 else tm, "mask_mean": tm_mean,
+                "weights_per_point": data["weight"], "profiles_per_point": data["profile"],
+            }
+    return result
+
+
+def run_stage(config, raw_fields, points_um=None, *, uin=None, device="cuda", tails=True, count_per_axis=65,
+              slots=64, schedule=None, return_psf_3d=True, plan=None, timings=None, check=True):
+    """Fused optical stage: every product reduced on the device.
+
+    Returns the dictionary of ``assemble`` / maomi.optics.propagate with FP64
+    energies, v4 masks and site-averaged tails.  ``plan`` reuses an existing
+    ``OpticalPlan``; ``timings`` (a dict) receives per-phase seconds."""
+    import torch
+    from .backends.cuda.batched import OpticalPlan, trapezoid
+    _lib.require_cuda(device)
+    t0 = time.perf_counter()
+    if plan is None:
+        plan = OpticalPlan(config, raw_fields, uin=uin, device=device)
+    points = fixed_locations(config, count_per_axis) if points_um is None else np.asarray(points_um, float)
+    pts, off = plan.offsets(points)
+    P = len(pts)
+    with torch.inference_mode():
+        res = plan.run_sites(off, tail_per_site=False, slots=slots, schedule=schedule, check=check)
+        psf, energies, s1, s2 = plan.finalize_focal(res["focal"], psf=True, sums=True)
+        dev = plan.device
+        r = config.vres
+        prof, wts = [], []
+        for j in range(2):
+            axial = plan.axial["top" if j == 0 else "bottom"].astype(np.float64)
+            pj = res["profiles"][j] * torch.as_tensor(axial * config.ss ** 2, device=dev)
+            prof.append(pj)
+            wts.append((pj * torch.as_tensor(trapezoid(len(axial)), device=dev)).sum(1) * config.prop_um)
+        values = torch.stack([energies, wts[0], wts[1]] if tails else [energies], 1)
+        shape = tuple(np.round(np.array(config.volume_um[:2]) * r).astype(int))
+        p_dev, coef = v4_coefficients_device(pts * r, values, device=dev) if P > 1 else (None, None)
+        if P > 1:
+            masks = v4_evaluate_grid_device(p_dev, coef, *shape, device=dev)
+        else:
+            masks = values[0].reshape(1, 1, -1).expand(shape[0], shape[1], -1).contiguous()
+        convs = []
+        if tails:
+            rt = plan.tail_resample
+            X, Y = rt.shape
+            scratch = torch.empty(plan.n2 * plan.n2, dtype=torch.float64, device=dev)
+            for j in range(2):
+                conv = torch.empty((X, Y), dtype=torch.float64, device=dev)
+                imgs = res["images"][j]
+                _lib.call("mm_tail_finalize", _lib.ptr(imgs), imgs.shape[0], plan.n2, plan.n2, _lib.ptr(rt.mx),
+                          _lib.ptr(rt.my), X, Y, float(config.ss ** 4) / P, _lib.ptr(conv), _lib.ptr(scratch),
+                          _lib.stream_of(dev))
+                convs.append(conv)
+        # ---- host copies of the final products
+        masks_h = masks.cpu().numpy()
+        psf_abs = (s2 / P).cpu().numpy()
+        psf_raw = (s1 / P).cpu().numpy()
+        energies_h = energies.cpu().numpy()
+        psf_3d = psf.cpu().numpy() if return_psf_3d else None
+        prof_h = [p.cpu().numpy() for p in prof]
+        wts_h = [w.cpu().numpy() for w in wts]
+        convs_h = [c.cpu().numpy() for c in convs]
+        neg = float(-torch.clamp(psf, max=0).sum(dtype=torch.float64) / torch.clamp(s2.sum(), min=1e-30))
+    mask = masks_h[..., 0]
+    mean = float(mask.mean())
+    if not np.isfinite(mean) or mean <= 0:
+        raise ValueError("Nonpositive or invalid mean excitation energy")
+    result = {
+        "psf": psf_abs, "psf_raw": psf_raw, "psf_3d": psf_3d, "points_um": pts, "energies": energies_h,
+        "mask_raw": mask, "mask": mask / mean, "mask_mean": mean, "mask_mode": "matlab_v4",
+        "tails_computed": bool(tails), "unique_optical_paths": P,
+        "negative_resampling_mass_fraction": neg,
+    }
+    if tails:
+        for j, name in enumerate(("psfT", "psfB")):
+            z = plan.z_positions[0][plan.cut:] if j == 0 else plan.z_positions[2]
+            tm = masks_h[..., j + 1]
+            tm_mean = float(tm.mean())
+            result[name] = {
+                "convmask": convs_h[j], "weight": float(wts_h[j].mean()),
+                "psfZ": _psf_z(config, z, prof_h[j].sum(0)),
+                "mask_raw": tm, "mask": tm / tm_mean if tm_mean > 0 else tm, "mask_mean": tm_mean,
+                "weights_per_point": wts_h[j], "profiles_per_point": prof_h[j],
+            }
+    if timings is not None:
+        timings["stage"] = time.perf_counter() - t0
+    return result
+
+
+def run_fixed(config, volume=None, *, vessels=None, raw_fields=None, scatter=True, custom_phase=None,
+              phase_units="radians", phase_aperture="objective", input_pupil=None, beam_weights=None, tails=True,
+              batch_size=32, count_per_axis=65, mask_mode="matlab_v4", device="cuda", rana=False,
+              render_image=False):
+    """Optical stage on the fixed lattice (maomi/fixed.py:193-411 without the
+    input-generation and static-scan stages, which lie outside this package).
+
+    ``raw_fields`` must be supplied; ``render_image`` and ``rana`` belong to the
+    downstream renderer and are not provided here."""
+    from .optics import pupil
+    if mask_mode != "matlab_v4":
+        raise ValueError("run_fixed requires matlab_v4")
+    if raw_fields is None:
+        raise ValueError("raw_fields are required (scattering-field generation is not part of this package)")
+    if render_image or (rana is not False and rana is not None):
+        raise ValueError("static scanning and RANA rendering are not part of run_fixed here; "
+                         "use maomi_b200.rana for the local-PSF renderer")
+    if beam_weights is not None:
+        raise ValueError("beam_weights requires a mapping of pupils")
+    if not isinstance(batch_size, int) or batch_size < 1:
+        raise ValueError("batch_size must be a positive integer")
+    if input_pupil is not None and custom_phase is not None:
+        raise ValueError("Supply either input_pupil or custom_phase; compose the field explicitly")
+    expected = field_shapes(config)
+    if len(raw_fields) != 3 or any(tuple(np.shape(a)) != tuple(s) for a, s in zip(raw_fields, expected)):
+        raise ValueError(f"Raw A/B/C fields must have shapes {expected}")
+    if any(np.iscomplexobj(a) or not np.isfinite(np.asarray(a)).all() for a in raw_fields):
+        raise ValueError("Raw refractive-index fields must be finite and real")
+    _lib.require_cuda(device)
+    import torch
+    started = time.perf_counter()
+    timings = {}
+    t = time.perf_counter()
+    u = (pupil(config, custom_phase=custom_phase, phase_units=phase_units, phase_aperture=phase_aperture,
+               device=device) if input_pupil is None
+         else torch.as_tensor(input_pupil, dtype=torch.complex64, device=device))
+    from .backends.cuda.batched import OpticalPlan
+    plan = OpticalPlan(config, raw_fields, uin=u, device=device)
+    torch.cuda.synchronize(device)
+    timings["plan"] = time.perf_counter() - t
+    t = time.perf_counter()
+    result = run_stage(config, raw_fields, fixed_locations(config, count_per_axis), device=device, tails=tails,
+                       slots=max(batch_size, 1), plan=plan)
+    timings["propagation_and_aggregation"] = time.perf_counter() - t
+    result["timing_seconds"] = timings
+    result["total_seconds"] = time.perf_counter() - started
+    result["settings"] = {"seed": config.seed, "scaling": config.scaling, "fields": "provided",
+                          "phase_units": phase_units, "phase_aperture": phase_aperture,
+                          "input_pupil": "provided" if input_pupil is not None else "gaussian",
+                          "count_per_axis": count_per_axis, "mask_mode": mask_mode,
+                          "psf_average": "arithmetic mean of absolute per-point PSFs"}
+    return result

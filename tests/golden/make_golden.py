@@ -1,0 +1,245 @@
+"""Generate golden fixtures by running the REFERENCE implementation (MaoMi 0.8.0b1).
+
+Run in a container where the reference source tree is mounted read-only:
+
+    python tests/golden/make_golden.py /root/reference
+
+It imports the reference package from that path (no bytecode is written),
+runs its CPU optical stage (``maomi.optics.propagate``, ``v4_interpolate``,
+``resize_xy``, ``translate_xy``, ``pupil``) and its local
+PSF operator (``maomi.rana.RanaOperator``) on seeded inputs, and stores inputs
+(where small) and outputs as ``*.npz`` next to this script.  Large inputs are
+regenerated from their seeds by ``maomi_b200.synthetic`` and stored only as a
+checksum.  The fixtures are what the tests use on machines without the
+reference tree.
+"""
+
+import sys
+from dataclasses import asdict
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+REPO = HERE.parents[1]
+
+
+def _import_reference(path):
+    sys.dont_write_bytecode = True
+    sys.path.insert(0, str(path))
+    sys.path.insert(0, str(REPO))
+    import torch  # noqa: F401  (the reference needs it)
+    import maomi  # noqa: F401
+    return torch
+
+
+def _cfg_dict(cfg):
+    d = asdict(cfg)
+    return {k: np.asarray(v) for k, v in d.items()}
+
+
+def _flat_result(prefix, out):
+    flat = {}
+    for k in ("psf_3d", "psf_raw", "psf", "mask_raw", "mask", "energies"):
+        flat[f"{prefix}{k}"] = np.asarray(out[k])
+    flat[f"{prefix}mask_mean"] = np.asarray(out["mask_mean"])
+    for t in ("psfT", "psfB"):
+        for k in ("convmask", "weight", "psfZ", "mask_raw", "mask_mean"):
+            flat[f"{prefix}{t}_{k}"] = np.asarray(out[t][k])
+    return flat
+
+
+def run_stage(torch, cfg, raw, points, *, custom_phase=None, fp64_too=True):
+    """Reference CPU stage in FP32 and (optionally) FP64; returns flat dict."""
+    from maomi.optics import propagate, pupil
+    res = {}
+    u32 = pupil(cfg, custom_phase=custom_phase, device="cpu") if custom_phase is not None else pupil(cfg)
+    res["pupil32"] = u32.numpy()
+    out = propagate(cfg, raw, points, uin=u32, device="cpu")
+    res.update(_flat_result("f32_", out))
+    if fp64_too:
+        old = torch.get_default_dtype()
+        torch.set_default_dtype(torch.float64)
+        try:
+            u64 = pupil(cfg, custom_phase=custom_phase, device="cpu") if custom_phase is not None else pupil(cfg)
+            res["pupil64"] = u64.numpy()
+            raw64 = [np.asarray(a, np.float64) for a in raw]
+            out = propagate(cfg, raw64, points, uin=u64.to(torch.complex128), device="cpu")
+            res.update(_flat_result("f64_", out))
+        finally:
+            torch.set_default_dtype(old)
+    return res
+
+
+def make_stage_small(torch):
+    from maomi.optics import OpticalConfig
+    from maomi.fixed import field_shapes, fixed_locations
+    from maomi_b200 import synthetic
+    cfg = synthetic.small_stage_config(OpticalConfig)
+    shapes = field_shapes(cfg)
+    raw = synthetic.raw_fields(cfg, shapes, sigma=2.0, rms=0.01, seed=1)
+    pts = fixed_locations(cfg, 3)
+    res = run_stage(torch, cfg, raw, pts)
+    res.update(points=pts, raw_seed=np.asarray(1), raw_sigma=np.asarray(2.0), raw_rms=np.asarray(0.01),
+               raw_checksum=np.asarray([float(np.sum(a, dtype=np.float64)) for a in raw]))
+    res.update({"cfg_" + k: v for k, v in _cfg_dict(cfg).items()})
+    return res
+
+
+def make_stage_reftest(torch):
+    """The reference's own GPU-vs-CPU test geometry (n=112, n2=72, ss=2)."""
+    from dataclasses import replace
+    from maomi.optics import OpticalConfig, prepare_fields, locations
+    cfg = OpticalConfig(volume_um=(16.0, 16.0, 10.0), depth_um=20.0, tail_um=10.0)
+    pts = locations(cfg.volume_um, 3)
+    phase = np.zeros((17, 17), np.float32)
+    phase[5:11, 5:11] = 0.2
+    res = {}
+    raw0 = [a.numpy() for a in prepare_fields(cfg, scatter=False)]
+    out = run_stage(torch, cfg, raw0, pts, custom_phase=phase)
+    res.update({"flat_" + k: v for k, v in out.items()})
+    raw1 = [a.numpy() for a in prepare_fields(cfg, scatter=True)]
+    for i, a in enumerate(raw1):
+        res[f"raw{i}"] = a
+    for mode in ("two-photon", "three-photon", "temporal-focusing"):
+        c = replace(cfg, scaling=mode)
+        out = run_stage(torch, c, raw1, pts, custom_phase=phase)
+        res.update({f"{mode}_" + k: v for k, v in out.items()})
+    res.update(points=pts, custom_phase=phase)
+    res.update({"cfg_" + k: v for k, v in _cfg_dict(cfg).items()})
+    return res
+
+
+def make_stage_bench_sites(torch):
+    """Benchmark geometry (n=256, 60 screens, Zernike pupil) on three sites."""
+    from maomi.optics import OpticalConfig, pupil
+    from maomi.optics import propagate
+    from maomi.fixed import field_shapes
+    from maomi_b200 import synthetic
+    cfg = synthetic.benchmark_stage_config(OpticalConfig)
+    shapes = field_shapes(cfg)
+    raw = synthetic.raw_fields(cfg, shapes, sigma=3.0, rms=0.015, seed=7)
+    pts = np.array([[0.0, 0.0], [128.0, 128.0], [252.0, 4.0]])
+    res = {}
+    u32 = pupil(cfg)
+    res["pupil32"] = u32.numpy()
+    out = propagate(cfg, raw, pts, uin=u32, device="cpu")
+    res.update(_flat_result("f32_", out))
+    old = torch.get_default_dtype()
+    torch.set_default_dtype(torch.float64)
+    try:
+        u64 = pupil(cfg)
+        res["pupil64"] = u64.numpy()
+        out = propagate(cfg, [np.asarray(a, np.float64) for a in raw], pts,
+                        uin=u64.to(torch.complex128), device="cpu")
+        res.update(_flat_result("f64_", out))
+    finally:
+        torch.set_default_dtype(old)
+    # Three sites make a degenerate v4 mask and the pupils are pinned in the
+    # numerics fixture: keep only the per-site products.
+    for k in list(res):
+        if k.startswith("pupil") or "mask" in k or k.endswith(("psf_raw", "_psf")):
+            del res[k]
+    res.update(points=pts, raw_seed=np.asarray(7), raw_sigma=np.asarray(3.0), raw_rms=np.asarray(0.015),
+               raw_checksum=np.asarray([float(np.sum(a, dtype=np.float64)) for a in raw]))
+    res.update({"cfg_" + k: v for k, v in _cfg_dict(cfg).items()})
+    return res
+
+
+def make_numerics(torch):
+    from maomi.numerics import resize_xy, translate_xy, v4_interpolate
+    from maomi._propagation import edge_apodization
+    from maomi.excitation import axial_profile
+    from maomi.optics import OpticalConfig
+    rng = np.random.default_rng(12)
+    res = {}
+    a = rng.standard_normal((20, 18, 3)).astype(np.float32)
+    res["resize_in"] = a
+    for s in (2, 0.5, 3):
+        res[f"resize_{s}"] = resize_xy(torch.as_tensor(a), s).numpy()
+        res[f"resize64_{s}"] = resize_xy(torch.as_tensor(a.astype(np.float64)), s).numpy()
+    for sh in (0.5, 1.0, 0.0):
+        res[f"translate_{sh}"] = translate_xy(torch.as_tensor(a.astype(np.float64)), sh).numpy()
+    res["edge_64"] = edge_apodization(64, "cpu", torch.float64).numpy()
+    res["edge_32"] = edge_apodization(64, "cpu", torch.float32).numpy()
+    # Zernike-aberrated pupils (modes 4-11) on a 96-point grid, both precisions
+    from maomi.optics import pupil
+    from maomi_b200 import synthetic
+    from dataclasses import replace
+    zc = OpticalConfig(volume_um=(16.0, 16.0, 10.0), depth_um=12.0, vres=1.0, ss=1)
+    zc = replace(zc, zernike_weights=synthetic.zernike_weights(zc, 3))
+    res["zpupil32"] = pupil(zc).numpy()
+    old = torch.get_default_dtype()
+    torch.set_default_dtype(torch.float64)
+    try:
+        res["zpupil64"] = pupil(zc).numpy()
+    finally:
+        torch.set_default_dtype(old)
+    res.update({"zcfg_" + k: v for k, v in _cfg_dict(zc).items()})
+    cfg = OpticalConfig(scaling="temporal-focusing")
+    for part, size in (("focus", 20), ("top", 7), ("bottom", 5)):
+        res[f"axial_{part}"] = axial_profile(cfg, size, part)
+    # v4: the reference test's data (tests/test_interpolation.py:21-25)
+    rng = np.random.default_rng(471)
+    pts = rng.uniform(-20, 20, (37, 2))
+    q = np.concatenate((pts, rng.uniform(-25, 25, (105, 2))))
+    vals = rng.uniform(.2, 2, (37, 4))
+    res.update(v4_points=pts, v4_queries=q, v4_values=vals,
+               v4_out=v4_interpolate(pts, vals, q, chunk=19, backend="cpu"))
+    # a lattice case shaped like mask assembly (9x9 sites -> 64x64 pixels)
+    lat = np.stack(np.meshgrid(np.arange(9) * 8.0, np.arange(9) * 8.0, indexing="ij"), -1).reshape(-1, 2)
+    lv = rng.uniform(.5, 2, (81, 3))
+    lq = np.stack(np.meshgrid(np.arange(64) + .5, np.arange(64) + .5, indexing="ij"), -1)
+    res.update(v4l_points=lat, v4l_values=lv, v4l_out=v4_interpolate(lat, lv, lq, backend="cpu"))
+    return res
+
+
+def make_local_fft(torch):
+    from maomi.rana import FullFieldPSF, DepthPSFBank, RanaOperator
+    from maomi.rana._fft import LocalFFTPlan
+    from maomi.rana.operator import _axis_weights
+    rng = np.random.default_rng(631)
+    res = {}
+    # (a) small native-style field, reference test fixture shapes
+    vol = rng.uniform(0, 1, (12, 14, 9))
+    k = rng.uniform(.1, 1, (2, 2, 3, 4, 3))
+    res.update(a_volume=vol, a_kernels=k)
+    for name, op in (("excitation", "excitation"), ("detection", "detection")):
+        f = FullFieldPSF(k, [0, 12], [0, 14], (1., 1., 1.), 920., op)
+        R = RanaOperator(f, device="cpu")
+        res[f"a_{name}_static"] = R.static(vol)
+        res[f"a_{name}_slab1"] = R.scan_slab(vol[..., :3], scan_avg=1)
+        res[f"a_{name}_slab2"] = R.scan_slab(vol[..., :3], scan_avg=2)
+        Rn = RanaOperator(f, native=True, device="cpu")
+        res[f"a_{name}_native_static"] = Rn.static(vol)
+    # (b) mid-size: 48x40x10 volume, 4x3 nodes, 7x6x5 kernels, 2-depth bank, even/odd sizes
+    vol = rng.uniform(0, 2, (48, 40, 10))
+    kern = rng.uniform(.05, 1, (2, 4, 3, 7, 6, 5))
+    xs, ys = np.linspace(0, 48, 4), np.linspace(0, 40, 3)
+    res.update(b_volume=vol, b_kernels=kern, b_x=xs, b_y=ys, b_depths=np.array([0.0, 10.0]))
+    for op in ("excitation", "detection"):
+        fields = tuple(FullFieldPSF(kern[d], xs, ys, (1., 1., 1.), 920., op) for d in range(2))
+        bank = DepthPSFBank(np.array([0.0, 10.0]), fields)
+        R = RanaOperator(bank, device="cpu")
+        res[f"b_{op}_static"] = R.static(vol)
+        res[f"b_{op}_slab"] = R.scan_slab(vol[..., 2:7], z_start=2, scan_avg=1)
+    # (c) the weights helper
+    nodes = np.array([0.0, 3.0, 10.0, 12.0])
+    pos = np.linspace(-1, 13, 29)
+    res.update(c_nodes=nodes, c_pos=pos, c_weights=_axis_weights(nodes, pos))
+    return res
+
+
+def main(ref_path):
+    torch = _import_reference(ref_path)
+    torch.set_num_threads(8)
+    for name, fn in (("numerics", make_numerics), ("local_fft", make_local_fft),
+                     ("stage_small", make_stage_small), ("stage_reftest", make_stage_reftest),
+                     ("stage_bench_sites", make_stage_bench_sites)):
+        out = fn(torch)
+        np.savez_compressed(HERE / f"{name}.npz", **out)
+        print(name, sum(np.asarray(v).nbytes for v in out.values()) // 1024, "KiB raw")
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")

@@ -1,0 +1,153 @@
+"""CUDA optical stage vs the CPU oracle and the reference's golden outputs.
+
+Tolerance (north star): relative L2 <= 1e-5 against the FP64 reference for
+PSFs, masks and tails.  The CUDA path forms every large phase argument in
+FP64 and rounds once; FFT arithmetic is FP32."""
+
+import numpy as np
+import pytest
+
+from conftest import cfg_from, golden, rel_l2
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-5
+
+
+@pytest.fixture(scope="module")
+def small():
+    from oracle import optics as O
+    from maomi_b200 import synthetic
+    d = golden("stage_small")
+    cfg = cfg_from(d)
+    raw = synthetic.raw_fields(cfg, O.field_shapes(cfg), sigma=float(d["raw_sigma"]), rms=float(d["raw_rms"]),
+                               seed=int(d["raw_seed"]))
+    return d, cfg, raw
+
+
+def _stage_errors(out, d, prefix="f64_"):
+    errs = {k: rel_l2(out[k], d[prefix + k]) for k in ("psf_3d", "psf", "psf_raw", "mask_raw", "energies")}
+    for t in ("psfT", "psfB"):
+        for k in ("convmask", "weight", "psfZ", "mask_raw"):
+            errs[f"{t}.{k}"] = rel_l2(out[t][k], d[f"{prefix}{t}_{k}"])
+    return errs
+
+
+def test_pupil_fp64_zernike():
+    from maomi_b200.optics import pupil
+    d = golden("numerics")
+    cfg = cfg_from(d, "zcfg_")
+    u = pupil(cfg).cpu().numpy()
+    assert rel_l2(u, d["zpupil64"]) < 1e-6
+
+
+def test_small_stage_matches_reference_fp64(small):
+    from maomi_b200.fixed import run_stage
+    d, cfg, raw = small
+    out = run_stage(cfg, raw, d["points"])
+    errs = _stage_errors(out, d)
+    bad = {k: v for k, v in errs.items() if not v < TOL}
+    assert not bad, errs
+
+
+@pytest.mark.parametrize("schedule", ["persistent", "batched"])
+def test_schedules_agree(small, schedule):
+    from maomi_b200.fixed import run_stage
+    d, cfg, raw = small
+    ref = run_stage(cfg, raw, d["points"], schedule="persistent", slots=4)
+    out = run_stage(cfg, raw, d["points"], schedule=schedule, slots=2)
+    np.testing.assert_array_equal(out["psf_3d"], ref["psf_3d"])
+    assert rel_l2(out["psfT"]["convmask"], ref["psfT"]["convmask"]) < 1e-6
+    assert rel_l2(out["mask_raw"], ref["mask_raw"]) < 1e-12
+
+
+def test_evaluate_per_site_matches_oracle(small):
+    """OpticalPlan.evaluate schema and per-site products vs the FP64 oracle."""
+    from oracle import optics as O
+    from maomi_b200.backends.cuda.batched import OpticalPlan
+    d, cfg, raw = small
+    plan = OpticalPlan(cfg, raw)
+    out = plan.evaluate(d["points"], batch_size=4, tails=True)
+    ref = O.propagate_sites(cfg, [np.asarray(a, np.float64) for a in raw], d["points"], O.pupil(cfg, np.float64))
+    assert out["psfs"].shape == ref["psfs"].shape and out["psfs"].dtype == np.float32
+    assert rel_l2(out["psfs"], ref["psfs"]) < TOL
+    for j, name in enumerate(("top", "bottom")):
+        assert rel_l2(out[name]["convmask"], ref["convmasks"][j]) < TOL
+        assert rel_l2(out[name]["weight"], ref["weights"][j]) < TOL
+        assert rel_l2(out[name]["profile"], ref["profiles"][j]) < TOL
+    assert plan.paths_evaluated == len(d["points"])
+
+
+def test_benchmark_geometry_matches_reference_fp64():
+    """256x256 windows, 60 screens, Zernike pupil: three sites vs the reference."""
+    from oracle import optics as O
+    from maomi_b200 import synthetic
+    from maomi_b200.backends.cuda.batched import OpticalPlan
+    d = golden("stage_bench_sites")
+    cfg = cfg_from(d)
+    raw = synthetic.raw_fields(cfg, O.field_shapes(cfg), sigma=float(d["raw_sigma"]), rms=float(d["raw_rms"]),
+                               seed=int(d["raw_seed"]))
+    plan = OpticalPlan(cfg, raw)
+    out = plan.evaluate(d["points"], batch_size=3, tails=True)
+    assert rel_l2(out["psfs"], d["f64_psf_3d"]) < TOL
+    assert rel_l2(out["psfs"].sum((1, 2, 3), dtype=np.float64), d["f64_energies"]) < TOL
+
+
+def test_v4_matches_reference():
+    from maomi_b200.numerics import v4_interpolate
+    from maomi_b200.backends.cuda.interpolation import evaluate_v4
+    d = golden("numerics")
+    np.testing.assert_allclose(v4_interpolate(d["v4_points"], d["v4_values"], d["v4_queries"]), d["v4_out"],
+                               rtol=1e-9, atol=1e-10)
+    q = d["v4_queries"].reshape(2, 71, 2)
+    np.testing.assert_allclose(v4_interpolate(d["v4_points"], d["v4_values"][:, :3], q),
+                               d["v4_out"][:, :3].reshape(2, 71, 3), rtol=1e-9, atol=1e-10)
+    lq = np.stack(np.meshgrid(np.arange(64) + .5, np.arange(64) + .5, indexing="ij"), -1)
+    np.testing.assert_allclose(v4_interpolate(d["v4l_points"], d["v4l_values"], lq), d["v4l_out"], rtol=1e-9,
+                               atol=1e-10)
+    from oracle.optics import v4_coefficients
+    c = v4_coefficients(d["v4_points"], d["v4_values"])
+    np.testing.assert_allclose(evaluate_v4(d["v4_points"], c, d["v4_queries"]), d["v4_out"], rtol=1e-9, atol=1e-10)
+    # edge cases of numerics.py:116-120
+    one = v4_interpolate([[3, 4]], [[2, 7]], np.zeros((5, 6, 2)))
+    np.testing.assert_array_equal(one, np.broadcast_to([2, 7], (5, 6, 2)))
+    assert v4_interpolate(d["v4_points"], d["v4_values"], np.empty((0, 2))).shape == (0, 4)
+
+
+def test_gather_and_resample_plan():
+    import torch
+    from oracle.optics import resample_matrix
+    from maomi_b200.backends.cuda.native import ResamplePlan, gather
+    rng = np.random.default_rng(5)
+    src = (rng.standard_normal((3, 40, 44)) + 1j * rng.standard_normal((3, 40, 44))).astype(np.complex64)
+    edge = rng.uniform(0.5, 1, (16, 16)).astype(np.float32)
+    off = np.array([[0, 0], [24, 28], [5, 9]], np.int32)
+    out = gather(torch.as_tensor(src, device="cuda"), torch.as_tensor(edge, device="cuda"), off, 16).cpu().numpy()
+    for b, (x, y) in enumerate(off):
+        np.testing.assert_array_equal(out[b], src[:, x:x + 16, y:y + 16] * edge)
+    field = (rng.standard_normal((2, 4, 24, 24)) + 1j * rng.standard_normal((2, 4, 24, 24))).astype(np.complex64)
+    axial = rng.uniform(0.5, 1, 4).astype(np.float32)
+    for ss, order in ((2, 2), (3, 1), (1, 3)):
+        rp = ResamplePlan(24, 24, ss, "cuda")
+        got = rp(torch.as_tensor(field, device="cuda"), 1.7, order=order, axial=axial).cpu().numpy()
+        m = resample_matrix(24, ss)
+        p = np.abs(field.astype(np.complex128)) ** (2 * order)
+        ref = np.einsum("xh,bzhw,yw->bxyz", m, p, m) * 1.7 * axial
+        assert rel_l2(got, ref) < 1e-6
+
+
+def test_full_size_translation_invariance():
+    """Benchmark geometry, 4,225 sites, zero screens: every site sees the same
+    optics, so all PSFs coincide and the v4 mask is flat."""
+    from maomi_b200 import synthetic
+    from maomi_b200.fixed import field_shapes, run_stage
+    from maomi_b200.optics import OpticalConfig
+    cfg = synthetic.benchmark_stage_config(OpticalConfig)
+    raw = [np.zeros(s, np.float32) for s in field_shapes(cfg)]
+    out = run_stage(cfg, raw)
+    p = out["psf_3d"]
+    assert p.shape == (4225, 40, 40, 46)
+    np.testing.assert_array_equal(p, np.broadcast_to(p[0], p.shape))
+    np.testing.assert_allclose(out["mask"], 1.0, rtol=1e-9)
+    for t in ("psfT", "psfB"):
+        np.testing.assert_allclose(out[t]["mask"], 1.0, rtol=1e-9)
+        assert out[t]["weight"] > 0
