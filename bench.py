@@ -1,0 +1,304 @@
+"""Benchmark: the MaoMi optical stage at benchmark size on B200.
+
+Workload (one "step"): the full optical stage for a 512x512x60-voxel tissue
+block -- phase preparation of 60 screens (768x768), 65x65 = 4,225 sites on
+256x256 complex64 windows through 10+46+4 screens, both tails, focal PSF
+finalisation and the FP64 v4 mask assembly (4,225 points -> 512x512 x 3).
+Metric: propagated sites/s (higher is better).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+``value`` times the stage with inputs resident in HBM; ``e2e`` times the same
+stage through the public API with the raw fields copied from pinned host
+memory and every product (psf_3d, masks, tails) copied back each step.  Under
+torchrun every rank processes its own tissue block (weak scaling, no
+collective on the data path); ``value`` is all ranks' sites over the slowest
+rank's device time.  ``--impl reference`` times the reference algorithm's CPU
+implementation (the oracle restatement) on the host cores.
+"""
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+SITES = 4225
+SCREEN_STEPS = 60
+WINDOW = 256
+FOCAL_BYTES = 4 * 40 * 40 * 46
+# algorithmic bytes per site: per step one complex64 field read + write and one
+# complex64 screen read (24 n^2), plus the float32 focal PSF written once
+BYTES_PER_SITE = SCREEN_STEPS * 24 * WINDOW * WINDOW + FOCAL_BYTES
+METRIC = "propagated sites/s at 512^2x60 (plain optical stage incl. tails + v4 mask)"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--schedule", default="persistent", choices=["persistent", "batched"])
+    ap.add_argument("--slots", type=int, default=64)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-sites", type=int, default=8)
+    ap.add_argument("--sites", type=int, default=SITES, help="profile a subset of the lattice (not a bench line)")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64", "fp32"])
+    return ap.parse_args()
+
+
+def peaks():
+    try:
+        return json.loads((ROOT / "MEASURED_PEAKS.json").read_text()), "measured"
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+def workload(rank=0):
+    from maomi_b200 import synthetic
+    from maomi_b200.fixed import field_shapes
+    from maomi_b200.optics import OpticalConfig
+    cfg = synthetic.benchmark_stage_config(OpticalConfig)
+    raw = synthetic.raw_fields(cfg, field_shapes(cfg), sigma=3.0, rms=0.015, seed=7 + rank)
+    return cfg, raw
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = Path(os.environ.get("TMPDIR", "/tmp")) / f"mm_clocks_{os.getpid()}.csv"
+
+    def __enter__(self):
+        cmd = ["nvidia-smi", "-i", str(self.index), "--query-gpu=clocks.sm,clocks.max.sm,power.draw,"
+               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+               "--format=csv,noheader,nounits", "-lms", "100"]
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(cmd, stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.fh.close()
+
+    def summary(self):
+        if self.proc is None or not self.path.exists():
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        rows = []
+        for line in self.path.read_text().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) == 7:
+                rows.append(parts)
+        self.path.unlink(missing_ok=True)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[0]) for r in rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[3 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def cpu_baseline(sites, cores):
+    """The reference algorithm on the host cores: per-site propagation (FP32
+    oracle restatement, FFTs on all cores) for a sample of sites, plus one full
+    v4 mask assembly (4,225 points -> 512x512, 3 columns)."""
+    from oracle import optics as O
+    cfg, raw = workload()
+    O.FFT_WORKERS = cores
+    pts = O.fixed_locations(cfg)
+    sample = pts[np.linspace(0, len(pts) - 1, sites).astype(int)]
+    u = O.pupil(cfg, np.float32)
+    phases = O.phase_screens(cfg, raw, np.float32)
+    t0 = time.perf_counter()
+    O.propagate_sites(cfg, raw, sample, u, phases=phases)
+    t_site = (time.perf_counter() - t0) / sites
+    vals = np.random.default_rng(0).uniform(0.5, 2, (len(pts), 3))
+    q = np.stack(np.meshgrid(np.arange(512) + .5, np.arange(512) + .5, indexing="ij"), -1)
+    t0 = time.perf_counter()
+    O.v4_interpolate(pts * cfg.vres, vals, q)
+    t_v4 = time.perf_counter() - t0
+    return t_site, t_v4
+
+
+def run_reference(args):
+    """CPU arm: each step propagates ``--cpu-sites`` sites; the v4 assembly is
+    timed once and amortised over the 4,225-site stage."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    cores = os.cpu_count() or 1
+    from oracle import optics as O
+    cfg, raw = workload()
+    O.FFT_WORKERS = cores
+    pts = O.fixed_locations(cfg)
+    u = O.pupil(cfg, np.float32)
+    phases = O.phase_screens(cfg, raw, np.float32)
+    times = []
+    for i in range(args.warmup + args.steps):
+        sample = pts[(np.arange(args.cpu_sites) * 97 + i * 13) % len(pts)]
+        t0 = time.perf_counter()
+        O.propagate_sites(cfg, raw, sample, u, phases=phases)
+        if i >= args.warmup:
+            times.append((time.perf_counter() - t0) / args.cpu_sites)
+    vals = np.random.default_rng(0).uniform(0.5, 2, (len(pts), 3))
+    q = np.stack(np.meshgrid(np.arange(512) + .5, np.arange(512) + .5, indexing="ij"), -1)
+    t0 = time.perf_counter()
+    O.v4_interpolate(pts * cfg.vres, vals, q)
+    t_v4 = time.perf_counter() - t0
+    t_site = float(np.mean(times))
+    stage = SITES * t_site + t_v4
+    value = SITES / stage
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "sites/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": stage * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "c64", "data": "synthetic",
+        "config": {"workload": "optical stage, 4,225 sites, 256^2 windows x 60 screens, 512^2 v4 mask",
+                   "sites": SITES, "window": WINDOW, "screens": SCREEN_STEPS},
+        "cpu_baseline": {"value": value, "unit": "sites/s", "cores": cores, "kind": "port",
+                         "sample": f"{args.cpu_sites} sites per step x {args.steps} steps of per-site propagation "
+                                   f"(FP32 NumPy/SciPy restatement of maomi.optics.propagate, FFTs on {cores} "
+                                   f"threads) + one full 4,225-point v4 assembly ({t_v4:.2f} s), extrapolated "
+                                   "to the 4,225-site stage"},
+        "e2e": {"value": value, "unit": "sites/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    import torch
+    import torch.distributed as dist
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = f"cuda:{local}"
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device(dev))
+    from maomi_b200 import _lib
+    from maomi_b200.fixed import stage_device, stage_to_host
+    lib = _lib.load()
+    cfg, raw = workload(rank)
+    raw_pinned = [torch.from_numpy(a).pin_memory() for a in raw]
+    raw_dev = [a.to(dev) for a in raw_pinned]
+    stream = torch.cuda.current_stream(dev)
+
+    from maomi_b200.fixed import fixed_locations
+    points = fixed_locations(cfg)[:args.sites]
+
+    def step(inputs, events=None):
+        return stage_device(cfg, inputs, points, device=dev, slots=args.slots, schedule=args.schedule, check=False,
+                            events=events, precision=args.precision)
+
+    # ---- device-resident timing
+    for _ in range(args.warmup):
+        step(raw_dev)
+    torch.cuda.synchronize(dev)
+    kev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    launches0 = lib.mm_launch_count()
+    with Clocks(local) as clk:
+        start.record(stream)
+        for i in range(args.steps):
+            step(raw_dev, events=kev[i])
+        stop.record(stream)
+        torch.cuda.synchronize(dev)
+    launches = (lib.mm_launch_count() - launches0) / args.steps
+    if world > 1:
+        dist.barrier()
+    ms = start.elapsed_time(stop) / args.steps
+    kernel_ms = float(np.mean([a.elapsed_time(b) for a, b in kev]))
+    if args.no_e2e:
+        if rank == 0:
+            print(json.dumps({"profile_case": True, "sites": len(points), "ms_per_step": ms, "kernel_ms": kernel_ms}))
+        return
+    # ---- end to end through the public API with host buffers
+    probe = step(raw_dev)
+    pinned = {k: torch.empty(v.shape, dtype=v.dtype, pin_memory=True) for k, v in
+              (("masks", probe["masks"]), ("psf_3d", probe["psf_3d"]))}
+    h2d = sum(a.numel() * a.element_size() for a in raw_pinned)
+    d2h = sum(v.numel() * v.element_size() for v in pinned.values())
+    e_start, e_stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    e_start.record(stream)
+    for _ in range(args.steps):
+        inputs = [a.to(dev, non_blocking=True) for a in raw_pinned]
+        res = stage_to_host(cfg, step(inputs), out=pinned)
+    e_stop.record(stream)
+    torch.cuda.synchronize(dev)
+    e2e_ms = e_start.elapsed_time(e_stop) / args.steps
+    d2h += sum(np.asarray(res[k]).nbytes for k in ("psf", "psf_raw", "energies")) + sum(
+        np.asarray(res[t][k]).nbytes for t in ("psfT", "psfB") for k in ("convmask", "weights_per_point",
+                                                                          "profiles_per_point"))
+    times = torch.tensor([ms, e2e_ms, kernel_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(times, op=dist.ReduceOp.MAX)
+    ms, e2e_ms, kernel_ms = [float(v) for v in times.cpu()]
+    pk, pk_kind = peaks()
+    achieved = len(points) * BYTES_PER_SITE / (kernel_ms * 1e-3) / 1e9
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": world * len(points) / (ms * 1e-3), "unit": "sites/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "c64", "data": "synthetic",
+            "config": {"workload": "optical stage, 4,225 sites, 256^2 windows x 60 screens (10+46+4), both "
+                                   "tails, 512^2 v4 mask", "sites": SITES, "window": WINDOW,
+                       "screens": SCREEN_STEPS, "schedule": args.schedule, "sites_in_flight": args.slots,
+                       "line_arithmetic": args.precision,
+                       "l2": "inputs larger than L2 (raw 141 MB + screens 283 MB per step)",
+                       "parallelism": f"{world} independent tissue blocks (one per GPU)"},
+            "e2e": {"value": world * len(points) / (e2e_ms * 1e-3), "unit": "sites/s", "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h)},
+            "gpu_launches": int(round(launches)),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
+                         "frac": achieved / pk["hbm_gbs"], "traffic": None,
+                         "kernel": "mm propagation (persistent)", "kernel_ms": kernel_ms,
+                         "bytes_per_launch": len(points) * BYTES_PER_SITE, "peak_source": pk_kind},
+            "clocks": clk.summary(),
+        }
+        if not args.no_cpu_baseline and world == 1:
+            cores = os.cpu_count() or 1
+            t_site, t_v4 = cpu_baseline(args.cpu_sites, cores)
+            v = SITES / (SITES * t_site + t_v4)
+            line["cpu_baseline"] = {"value": v, "unit": "sites/s", "cores": cores, "kind": "port",
+                                    "sample": f"{args.cpu_sites} sites propagated (FP32 oracle, {cores} FFT threads,"
+                                              f" {t_site:.3f} s/site) + one full v4 assembly ({t_v4:.2f} s), "
+                                              "extrapolated to 4,225 sites"}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

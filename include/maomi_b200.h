@@ -39,6 +39,9 @@ const char* mm_last_error(void);
 /* 1 if the current device is an sm_100 part the library was built for. */
 int mm_device_supported(void);
 
+/* Kernels launched by this library since it was loaded (all threads). */
+unsigned long long mm_launch_count(void);
+
 /* ------------------------------------------------------------------------
  * Screen gather: dst[b,z,x,y] = src[z, off[b,0]+x, off[b,1]+y] * edge[x*N+y]
  * Replaces gather_screens, maomi/backends/cuda/optical_kernels.cu:3-12
@@ -172,7 +175,13 @@ typedef struct {
                               zeroed by the call                                  */
   const int32_t* offsets;  /* (P,2) window offsets on the screen lattice          */
   int nsites;
+  int precision;           /* arithmetic of the radix-2 line transforms: FP32,
+                              FP64 (butterflies, twiddles and filter in FP64) or
+                              MIXED (forward FP32, inverse FP64); the field is
+                              stored complex64 in every mode                      */
 } mm_stage_plan;
+
+enum { MM_PRECISION_FP32 = 0, MM_PRECISION_FP64 = 1, MM_PRECISION_MIXED = 2 };
 
 enum { MM_SCHEDULE_PERSISTENT = 0, MM_SCHEDULE_BATCHED = 1 };
 

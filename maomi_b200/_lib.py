@@ -14,6 +14,8 @@ LIB_PATH = Path(__file__).resolve().parent / "libmaomi_b200.so"
 
 MM_OK, MM_ERR_ARGUMENT, MM_ERR_CUDA, MM_ERR_TIMEOUT, MM_ERR_NONFINITE, MM_ERR_UNSUPPORTED = 0, -1, -2, -3, -4, -5
 MM_SCHEDULE_PERSISTENT, MM_SCHEDULE_BATCHED = 0, 1
+MM_PRECISION_FP32, MM_PRECISION_FP64, MM_PRECISION_MIXED = 0, 1, 2
+PRECISIONS = {"fp32": MM_PRECISION_FP32, "fp64": MM_PRECISION_FP64, "mixed": MM_PRECISION_MIXED}
 
 c_int_p = POINTER(c_int)
 c_float_p = POINTER(c_float)
@@ -29,7 +31,8 @@ class StagePlan(Structure):
     _fields_ = [("stage", StageDesc * 3), ("base", c_void_p), ("n", c_int), ("n2", c_int), ("order", c_int),
                 ("cut", c_int), ("focal_x0", c_int), ("focal_y0", c_int), ("focal_h", c_int), ("focal_w", c_int),
                 ("tail_weight", c_void_p * 2), ("focal", c_void_p), ("tail_image", c_void_p * 2),
-                ("tail_per_site", c_int), ("tail_profile", c_void_p * 2), ("offsets", c_void_p), ("nsites", c_int)]
+                ("tail_per_site", c_int), ("tail_profile", c_void_p * 2), ("offsets", c_void_p), ("nsites", c_int),
+                ("precision", c_int)]
 
 
 class PupilDesc(Structure):
@@ -56,6 +59,7 @@ SIGNATURES = {
     "mm_version": (c_int, []),
     "mm_last_error": (c_char_p, []),
     "mm_device_supported": (c_int, []),
+    "mm_launch_count": (ctypes.c_ulonglong, []),
     "mm_gather_screens": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int, c_int, c_int, c_int, c_void_p]),
     "mm_resample_power": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int,
                                   c_int, c_int, c_int, c_int, c_int, c_int, c_int, c_float, c_void_p]),

@@ -21,16 +21,25 @@ from ...numerics import is_identity_table, resample_matrix, resize_table, sparse
 from ...optics import pupil
 
 
-def transfer_kernels(z, size, d2, wvl, nr):
+FFT_SIZES = (64, 128, 256, 512)
+
+
+def transfer_kernels(z, size, d2, wvl, nr, *, circulant=None):
     """Per-step 1-D transfer functions in FFT order with 1/size folded in:
-    exp(-1j*pi*(wvl/nr)*dz*(k/(size*d2))^2)/size, phases formed in FP64."""
+    exp(-1j*pi*(wvl/nr)*dz*(k/(size*d2))^2)/size, phases formed in FP64.
+
+    For windows without a radix-2 kernel (``circulant``, default: size not in
+    64..512 powers of two) the kernels are the equivalent circular-convolution
+    taps IDFT(Q), also formed in FP64."""
+    if circulant is None:
+        circulant = size not in FFT_SIZES
     lam = float(wvl) / float(nr)
     ks = np.fft.fftfreq(size) * size  # signed integer frequencies in FFT order
     f2 = (ks / (size * float(d2))) ** 2
     out = np.empty((len(z) - 1, size), np.complex64)
     for i, dz in enumerate(np.diff(np.asarray(z, float))):
-        phase = np.mod(-np.pi * lam * dz * f2, 2 * np.pi)
-        out[i] = (np.exp(1j * phase) / size).astype(np.complex64)
+        q = np.exp(1j * np.mod(-np.pi * lam * dz * f2, 2 * np.pi))
+        out[i] = (np.fft.ifft(q) if circulant else q / size).astype(np.complex64)
     return out
 
 
@@ -60,9 +69,15 @@ class ResampleTables:
 class OpticalPlan:
     """Persistent device state of the optical stage for one configuration."""
 
-    def __init__(self, config, raw_fields, *, uin=None, device="cuda", native=True):
+    def __init__(self, config, raw_fields, *, uin=None, device="cuda", native=True, precision="fp64"):
         import torch
         _lib.require_cuda(device)
+        if precision not in _lib.PRECISIONS:
+            raise ValueError("precision must be fp32, mixed or fp64")
+        #: arithmetic of the radix-2 line transforms: "fp64" (FP64 butterflies,
+        #: twiddles and filter), "mixed" (forward FP32, inverse FP64) or "fp32";
+        #: fields are stored complex64 in every mode
+        self.precision = precision
         self.config = copy.deepcopy(config)
         self.device = device
         self.native = native
@@ -153,7 +168,7 @@ class OpticalPlan:
         return _lib.MM_SCHEDULE_PERSISTENT if schedule == "persistent" else _lib.MM_SCHEDULE_BATCHED
 
     # ------------------------------------------------------------ propagation
-    def run_sites(self, offsets, *, tail_per_site, slots, schedule=None, check=True):
+    def run_sites(self, offsets, *, tail_per_site, slots, schedule=None, check=True, events=None):
         """Propagate every site; returns device buffers (focal, tail images, profiles)."""
         import torch
         dev = self.device
@@ -190,12 +205,17 @@ class OpticalPlan:
         plan.tail_profile[0], plan.tail_profile[1] = prof[0].data_ptr(), prof[1].data_ptr()
         plan.offsets = off.data_ptr()
         plan.nsites = P
+        plan.precision = _lib.PRECISIONS[self.precision]
         lib = _lib.load()
         wbytes = lib.mm_propagate_workspace_size(plan, slots, sched)
         work = torch.empty(wbytes + 256, dtype=torch.uint8, device=dev)
         base = (work.data_ptr() + 255) // 256 * 256
-        _lib.check(lib.mm_propagate_sites(plan, sched, slots, _lib.c_void_p(base), wbytes, int(check),
-                                          _lib.stream_of(dev)), "propagation")
+        if events is not None:
+            events[0].record()
+        rc = lib.mm_propagate_sites(plan, sched, slots, _lib.c_void_p(base), wbytes, int(check), _lib.stream_of(dev))
+        if events is not None:
+            events[1].record()
+        _lib.check(rc, "propagation")
         self.paths_evaluated += P
         return dict(focal=focal, images=imgs, profiles=prof, offsets=off, workspace=work)
 

@@ -1,4 +1,5 @@
 // Library-level entry points: version, error reporting, device check.
+#include <atomic>
 #include <string>
 
 #include "common.cuh"
@@ -7,7 +8,10 @@ namespace mm {
 
 namespace {
 thread_local std::string g_error;
+std::atomic<unsigned long long> g_launches{0};
 }
+
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
 void set_error(const char* fmt, ...) {
   char buf[1024];
@@ -28,6 +32,8 @@ int cuda_status(cudaError_t e, const char* what) {
 extern "C" int mm_version(void) { return 100; }
 
 extern "C" const char* mm_last_error(void) { return mm::g_error.c_str(); }
+
+extern "C" unsigned long long mm_launch_count(void) { return mm::g_launches.load(std::memory_order_relaxed); }
 
 extern "C" int mm_device_supported(void) {
   int dev = 0, major = 0, minor = 0;

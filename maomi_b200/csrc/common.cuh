@@ -14,6 +14,7 @@ namespace mm {
 // ----------------------------------------------------------------- errors --
 void set_error(const char* fmt, ...);
 int cuda_status(cudaError_t e, const char* what);
+void count_launch();
 
 #define MM_CHECK_ARG(cond, ...)                     \
   do {                                              \
@@ -29,7 +30,11 @@ int cuda_status(cudaError_t e, const char* what);
     if (e_ != cudaSuccess) return ::mm::cuda_status(e_, what);    \
   } while (0)
 
-#define MM_CHECK_LAUNCH(what) MM_CHECK_CUDA(cudaGetLastError(), what)
+#define MM_CHECK_LAUNCH(what)  \
+  do {                          \
+    ::mm::count_launch();       \
+    MM_CHECK_CUDA(cudaGetLastError(), what); \
+  } while (0)
 
 // ---------------------------------------------------------------- complex --
 __host__ __device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
@@ -40,10 +45,35 @@ __host__ __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
 __host__ __device__ __forceinline__ float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
 __host__ __device__ __forceinline__ float cnorm2(float2 a) { return a.x * a.x + a.y * a.y; }
 
+__host__ __device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__host__ __device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__host__ __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__host__ __device__ __forceinline__ double2 cmul(double2 a, float2 b) { return cmul(a, make_double2(b.x, b.y)); }
+__host__ __device__ __forceinline__ double cnorm2(double2 a) { return a.x * a.x + a.y * a.y; }
+
+// Conversions between the storage type (float2) and a register type.
+template <class C> __device__ __forceinline__ C from_f2(float2 a);
+template <> __device__ __forceinline__ float2 from_f2<float2>(float2 a) { return a; }
+template <> __device__ __forceinline__ double2 from_f2<double2>(float2 a) { return make_double2(a.x, a.y); }
+__device__ __forceinline__ float2 to_f2(float2 a) { return a; }
+__device__ __forceinline__ float2 to_f2(double2 a) { return make_float2(float(a.x), float(a.y)); }
+template <class C> __device__ __forceinline__ C promote(float2 a) { return from_f2<C>(a); }
+template <class C> __device__ __forceinline__ C promote(double2 a);
+template <> __device__ __forceinline__ double2 promote<double2>(double2 a) { return a; }
+template <class C> __device__ __forceinline__ C make_c(double re, double im);
+template <> __device__ __forceinline__ float2 make_c<float2>(double re, double im) { return make_float2(float(re), float(im)); }
+template <> __device__ __forceinline__ double2 make_c<double2>(double re, double im) { return make_double2(re, im); }
+
 // a * (SIGN * i): SIGN = -1 is the forward-DFT quarter turn, +1 the inverse one.
 template <int SIGN>
 __device__ __forceinline__ float2 quarter(float2 a) {
   return SIGN < 0 ? make_float2(a.y, -a.x) : make_float2(-a.y, a.x);
+}
+template <int SIGN>
+__device__ __forceinline__ double2 quarter(double2 a) {
+  return SIGN < 0 ? make_double2(a.y, -a.x) : make_double2(-a.y, a.x);
 }
 
 // |E|^(2*order) as the reference resample kernel forms it: p = x^2+y^2, then
@@ -52,6 +82,19 @@ __device__ __forceinline__ float photon_power(float2 e, int order) {
   float p = cnorm2(e);
   return order == 1 ? p : (order == 2 ? p * p : p * p * p);
 }
+__device__ __forceinline__ float photon_power(double2 e, int order) {
+  const double p = cnorm2(e);
+  return float(order == 1 ? p : (order == 2 ? p * p : p * p * p));
+}
+
+// Asynchronous 8-byte global -> shared copy (L1-allocating), its commit and
+// the wait for all of this thread's outstanding copies.
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 // Acquire load of a counter written by other CTAs (GPU scope).
 __device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {

@@ -19,61 +19,70 @@
 
 namespace mm {
 
-// cos / sin of pi*k/16, k = 0..16 (exact values rounded once to float).
-__device__ constexpr float kCos16[17] = {
-    1.0f, 0.98078528040323043058f, 0.92387953251128673848f, 0.83146961230254523567f,
-    0.70710678118654752440f, 0.55557023301960222474f, 0.38268343236508977173f, 0.19509032201612826785f,
-    0.0f, -0.19509032201612826785f, -0.38268343236508977173f, -0.55557023301960222474f,
-    -0.70710678118654752440f, -0.83146961230254523567f, -0.92387953251128673848f, -0.98078528040323043058f,
-    -1.0f};
-__device__ constexpr float kSin16[17] = {
-    0.0f, 0.19509032201612826785f, 0.38268343236508977173f, 0.55557023301960222474f,
-    0.70710678118654752440f, 0.83146961230254523567f, 0.92387953251128673848f, 0.98078528040323043058f,
-    1.0f, 0.98078528040323043058f, 0.92387953251128673848f, 0.83146961230254523567f,
-    0.70710678118654752440f, 0.55557023301960222474f, 0.38268343236508977173f, 0.19509032201612826785f,
-    0.0f};
+// cos / sin of pi*k/16, k = 0..16 (exact values; rounded once to the
+// register precision where used).
+__device__ constexpr double kCos16[17] = {
+    1.0, 0.98078528040323043058, 0.92387953251128673848, 0.83146961230254523567,
+    0.70710678118654752440, 0.55557023301960222474, 0.38268343236508977173, 0.19509032201612826785,
+    0.0, -0.19509032201612826785, -0.38268343236508977173, -0.55557023301960222474,
+    -0.70710678118654752440, -0.83146961230254523567, -0.92387953251128673848, -0.98078528040323043058,
+    -1.0};
+__device__ constexpr double kSin16[17] = {
+    0.0, 0.19509032201612826785, 0.38268343236508977173, 0.55557023301960222474,
+    0.70710678118654752440, 0.83146961230254523567, 0.92387953251128673848, 0.98078528040323043058,
+    1.0, 0.98078528040323043058, 0.92387953251128673848, 0.83146961230254523567,
+    0.70710678118654752440, 0.55557023301960222474, 0.38268343236508977173, 0.19509032201612826785,
+    0.0};
+
+template <class C> struct Real;
+template <> struct Real<float2> { using T = float; };
+template <> struct Real<double2> { using T = double; };
 
 // a * W_32^k with W = exp(SIGN * 2*pi*i/32), k = 0..15 (angle pi*k/16).
-template <int SIGN, int K>
-__device__ __forceinline__ float2 rot32(float2 a) {
+template <int SIGN, int K, class C>
+__device__ __forceinline__ C rot32(C a) {
+  using T = typename Real<C>::T;
   if constexpr (K == 0) {
     return a;
   } else if constexpr (K == 8) {
     return quarter<SIGN>(a);
   } else {
-    const float c = kCos16[K], s = SIGN * kSin16[K];
-    return make_float2(a.x * c - a.y * s, a.x * s + a.y * c);
+    const T c = T(kCos16[K]), s = T(SIGN * kSin16[K]);
+    C r;
+    r.x = a.x * c - a.y * s;
+    r.y = a.x * s + a.y * c;
+    return r;
   }
 }
 
-template <int SIGN>
-__device__ __forceinline__ void dft2(float2* v) {
-  float2 a = v[0], b = v[1];
+template <int SIGN, class C>
+__device__ __forceinline__ void dft2(C* v) {
+  C a = v[0], b = v[1];
   v[0] = cadd(a, b);
   v[1] = csub(a, b);
 }
 
 // 4-point DFT on v[0], v[S], v[2S], v[3S] (natural order in and out).
-template <int SIGN, int S = 1>
-__device__ __forceinline__ void dft4s(float2* v) {
-  float2 t0 = cadd(v[0], v[2 * S]);
-  float2 t1 = csub(v[0], v[2 * S]);
-  float2 t2 = cadd(v[S], v[3 * S]);
-  float2 t3 = quarter<SIGN>(csub(v[S], v[3 * S]));
+template <int SIGN, int S = 1, class C>
+__device__ __forceinline__ void dft4s(C* v) {
+  C t0 = cadd(v[0], v[2 * S]);
+  C t1 = csub(v[0], v[2 * S]);
+  C t2 = cadd(v[S], v[3 * S]);
+  C t3 = quarter<SIGN>(csub(v[S], v[3 * S]));
   v[0] = cadd(t0, t2);
   v[2 * S] = csub(t0, t2);
   v[S] = cadd(t1, t3);
   v[3 * S] = csub(t1, t3);
 }
 
-template <int SIGN>
-__device__ __forceinline__ void dft4(float2* v) { dft4s<SIGN, 1>(v); }
+template <int SIGN, class C>
+__device__ __forceinline__ void dft4(C* v) { dft4s<SIGN, 1>(v); }
 
 // 8-point DFT: two interleaved 4-point DFTs and a radix-2 combine.
-template <int SIGN>
-__device__ __forceinline__ void dft8(float2* v) {
-  float2 e[4] = {v[0], v[2], v[4], v[6]};
-  float2 o[4] = {v[1], v[3], v[5], v[7]};
+template <int SIGN, class C>
+__device__ __forceinline__ void dft8(C* v) {
+  C e[4] = {v[0], v[2], v[4], v[6]};
+  C o[4] = {v[1], v[3], v[5], v[7]};
   dft4<SIGN>(e);
   dft4<SIGN>(o);
   o[1] = rot32<SIGN, 4>(o[1]);
@@ -87,8 +96,8 @@ __device__ __forceinline__ void dft8(float2* v) {
 }
 
 // 16-point DFT: radix-4 decimation in time (4 x 4 with W_16 twiddles).
-template <int SIGN>
-__device__ __forceinline__ void dft16(float2* v) {
+template <int SIGN, class C>
+__device__ __forceinline__ void dft16(C* v) {
   // F_r = DFT4(v[r], v[r+4], v[r+8], v[r+12]) computed in place (stride 4).
 #pragma unroll
   for (int r = 0; r < 4; ++r) dft4s<SIGN, 4>(v + r);
@@ -102,14 +111,16 @@ __device__ __forceinline__ void dft16(float2* v) {
   v[3 + 4 * 1] = rot32<SIGN, 6>(v[3 + 4 * 1]);
   v[3 + 4 * 2] = rot32<SIGN, 12>(v[3 + 4 * 2]);
   {  // W_16^9 = -W_16^1
-    float2 a = rot32<SIGN, 2>(v[3 + 4 * 3]);
-    v[3 + 4 * 3] = make_float2(-a.x, -a.y);
+    C a = rot32<SIGN, 2>(v[3 + 4 * 3]);
+    a.x = -a.x;
+    a.y = -a.y;
+    v[3 + 4 * 3] = a;
   }
   // X[k1 + 4*k2] = DFT4 over r of the twiddled F_r[k1]: rows of 4.
 #pragma unroll
   for (int k1 = 0; k1 < 4; ++k1) dft4s<SIGN, 1>(v + 4 * k1);
   // v[4*k1 + k2] holds X[k1 + 4*k2]: transpose the 4x4 index in registers.
-  float2 t[16];
+  C t[16];
 #pragma unroll
   for (int k1 = 0; k1 < 4; ++k1)
 #pragma unroll
@@ -119,9 +130,9 @@ __device__ __forceinline__ void dft16(float2* v) {
 }
 
 // 32-point DFT: radix-2 decimation in time over two 16-point DFTs.
-template <int SIGN>
-__device__ __forceinline__ void dft32(float2* v) {
-  float2 e[16], o[16];
+template <int SIGN, class C>
+__device__ __forceinline__ void dft32(C* v) {
+  C e[16], o[16];
 #pragma unroll
   for (int i = 0; i < 16; ++i) {
     e[i] = v[2 * i];
@@ -131,7 +142,7 @@ __device__ __forceinline__ void dft32(float2* v) {
   dft16<SIGN>(o);
 #pragma unroll
   for (int k = 0; k < 16; ++k) {
-    float2 w;
+    C w;
     switch (k) {  // resolved at compile time after unrolling
       case 0: w = o[k]; break;
       case 1: w = rot32<SIGN, 1>(o[k]); break;
@@ -155,8 +166,8 @@ __device__ __forceinline__ void dft32(float2* v) {
   }
 }
 
-template <int R, int SIGN>
-__device__ __forceinline__ void dft(float2* v) {
+template <int R, int SIGN, class C>
+__device__ __forceinline__ void dft(C* v) {
   static_assert(R == 2 || R == 4 || R == 8 || R == 16 || R == 32, "unsupported radix");
   if constexpr (R == 2) dft2<SIGN>(v);
   else if constexpr (R == 4) dft4<SIGN>(v);
@@ -170,55 +181,116 @@ __device__ __forceinline__ void dft(float2* v) {
 // exchange buffer: R1 rows of (R2 + 1) float2 (the +1 keeps the transposed
 // reads bank-conflict free).  Two buffers alternate so one barrier per
 // exchange suffices.
-template <int R1_, int R2_>
+//
+// CF / CI are the register arithmetic types of the forward and the inverse
+// half: float2 (FP32) or double2 (FP64 butterflies, twiddles and filter).
+// The line enters and leaves as complex64 and the exchanges are complex64.
+// The inverse half carries most of the rounding that reaches the saved
+// intensities, so <float2, double2> ("mixed") recovers most of the FP64
+// accuracy for half of its cost.
+template <int R1_, int R2_, class CF_ = float2, class CI_ = CF_>
 struct FftLine {
+  using CF = CF_;
+  using CI = CI_;
   static constexpr int R1 = R1_;
   static constexpr int R2 = R2_;
   static constexpr int N = R1 * R2;
   static constexpr int J = R1 / R2;  // columns of the second pass per thread
   static constexpr int PITCH = R2 + 1;
   static constexpr int XBUF = R1 * PITCH;  // float2 per line per buffer
+  static constexpr bool kFft = true;
+  static constexpr size_t kTwiddleBytes = (size_t)N * (sizeof(CF) + sizeof(CI));
   static_assert(R1 % R2 == 0, "R2 must divide R1");
 
-  // twf[k1*R2 + t] = W_N^(t*k1); twi[n*R1 + k1] = W_N^(-n*k1)   (shared memory)
-  __device__ static void propagate(float2 (&v)[R1], int t, const float2* __restrict__ q,
-                                   float2* xa, float2* xb, const float2* twf, const float2* twi) {
+  // twf[k1*R2 + t] = W_N^(t*k1) (CF);  twi[n*R1 + k1] = W_N^(-n*k1) (CI)
+  __device__ static void propagate(float2 (&x)[R1], int t, const float2* __restrict__ q, int /*n*/,
+                                   float2* xa, float2* xb, const CF* twf, const CI* twi) {
+    CF v[R1];
+#pragma unroll
+    for (int m = 0; m < R1; ++m) v[m] = from_f2<CF>(x[m]);
     // ---- forward pass 1: DFT over m of x[t + R2*m], twiddle, exchange
     dft<R1, -1>(v);
 #pragma unroll
     for (int k1 = 1; k1 < R1; ++k1) v[k1] = cmul(v[k1], twf[k1 * R2 + t]);
 #pragma unroll
-    for (int k1 = 0; k1 < R1; ++k1) xa[k1 * PITCH + t] = v[k1];
+    for (int k1 = 0; k1 < R1; ++k1) xa[k1 * PITCH + t] = to_f2(v[k1]);
     __syncthreads();
     // ---- forward pass 2: thread t owns k1 = t + R2*j
 #pragma unroll
     for (int j = 0; j < J; ++j)
 #pragma unroll
-      for (int n2 = 0; n2 < R2; ++n2) v[j * R2 + n2] = xa[(t + R2 * j) * PITCH + n2];
+      for (int n2 = 0; n2 < R2; ++n2) v[j * R2 + n2] = from_f2<CF>(xa[(t + R2 * j) * PITCH + n2]);
 #pragma unroll
     for (int j = 0; j < J; ++j) dft<R2, -1>(v + j * R2);
-    // v[j*R2 + k2] = X[k1 + R1*k2];  filter in FFT order
+    // v[j*R2 + k2] = X[k1 + R1*k2];  filter in FFT order (inverse precision)
+    CI w[R1];
 #pragma unroll
     for (int j = 0; j < J; ++j)
 #pragma unroll
-      for (int k2 = 0; k2 < R2; ++k2) v[j * R2 + k2] = cmul(v[j * R2 + k2], __ldg(q + t + R2 * j + R1 * k2));
+      for (int k2 = 0; k2 < R2; ++k2)
+        w[j * R2 + k2] = cmul(promote<CI>(v[j * R2 + k2]), __ldg(q + t + R2 * j + R1 * k2));
     // ---- inverse pass 1: IDFT over k2 -> n_a, twiddle W_N^(-n_a*k1), exchange
 #pragma unroll
-    for (int j = 0; j < J; ++j) dft<R2, +1>(v + j * R2);
+    for (int j = 0; j < J; ++j) dft<R2, +1>(w + j * R2);
 #pragma unroll
     for (int j = 0; j < J; ++j)
 #pragma unroll
       for (int na = 0; na < R2; ++na) {
         const int k1 = t + R2 * j;
-        float2 z = v[j * R2 + na];
+        CI z = w[j * R2 + na];
         if (na) z = cmul(z, twi[na * R1 + k1]);
-        xb[k1 * PITCH + na] = z;
+        xb[k1 * PITCH + na] = to_f2(z);
       }
     __syncthreads();
     // ---- inverse pass 2: thread t = n_a gathers every k1
 #pragma unroll
-    for (int k1 = 0; k1 < R1; ++k1) v[k1] = xb[k1 * PITCH + t];
-    dft<R1, +1>(v);
+    for (int k1 = 0; k1 < R1; ++k1) w[k1] = from_f2<CI>(xb[k1 * PITCH + t]);
+    dft<R1, +1>(w);
+#pragma unroll
+    for (int m = 0; m < R1; ++m) x[m] = to_f2(w[m]);
+  }
+};
+
+// --------------------------------------------------------------------------
+// Any line length n <= 16*RMAX: the step along the line is the circular
+// convolution with p = IDFT(Q) (one n-tap complex kernel per step, formed in
+// FP64 on the host), accumulated in FP64.  Used for window sizes without a
+// radix-2 factorisation (e.g. the 112 / 72 windows of supersampled configs).
+template <int RMAX>
+struct DenseLine {
+  using CF = float2;
+  using CI = float2;
+  static constexpr size_t kTwiddleBytes = 0;
+  static constexpr int R1 = RMAX;
+  static constexpr int R2 = 16;
+  static constexpr int N = RMAX * 16;  // capacity
+  static constexpr int XBUF = N;
+  static constexpr bool kFft = false;
+
+  __device__ static void propagate(float2 (&v)[R1], int t, const float2* __restrict__ ker, int n, float2* xa,
+                                   float2* /*xb*/, const CF* /*twf*/, const CI* /*twi*/) {
+#pragma unroll
+    for (int j = 0; j < R1; ++j) {
+      const int e = t + R2 * j;
+      if (e < n) xa[e] = v[j];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < R1; ++j) {
+      const int e = t + R2 * j;
+      if (e < n) {
+        double re = 0.0, im = 0.0;
+        for (int k = 0; k < n; ++k) {
+          int m = e - k;
+          m += m < 0 ? n : 0;
+          const float2 a = __ldg(ker + m), b = xa[k];
+          re += double(a.x) * b.x - double(a.y) * b.y;
+          im += double(a.x) * b.y + double(a.y) * b.x;
+        }
+        v[j] = make_float2(float(re), float(im));
+      }
+    }
+    __syncthreads();
   }
 };
 

@@ -235,20 +235,25 @@ __global__ void base_norm_kernel(float2* __restrict__ out, int total, const doub
 
 // One 1-D propagate along rows (axis 0) or columns (axis 1) of an n x n field.
 template <class L, int LINES>
-__global__ void __launch_bounds__(LINES * L::R2) line_pass_kernel(float2* __restrict__ f, int axis, const float2* __restrict__ q) {
+__global__ void __launch_bounds__(LINES * L::R2) line_pass_kernel(float2* __restrict__ f, int n, int axis,
+                                                                  const float2* __restrict__ q) {
   extern __shared__ float4 smem_raw[];
+  using CF = typename L::CF;
+  using CI = typename L::CI;
   float2* xa = reinterpret_cast<float2*>(smem_raw);
   float2* xb = xa + LINES * L::XBUF;
-  float2* twf = xb + LINES * L::XBUF;
-  float2* twi = twf + L::N;
-  for (int i = threadIdx.x; i < L::N; i += blockDim.x) {
-    double s, c;
-    const int k1 = i / L::R2, t = i % L::R2;
-    sincospi(-2.0 * double((t * k1) % L::N) / L::N, &s, &c);
-    twf[i] = make_float2(float(c), float(s));
-    const int nn = i / L::R1, k2 = i % L::R1;
-    sincospi(2.0 * double((nn * k2) % L::N) / L::N, &s, &c);
-    twi[i] = make_float2(float(c), float(s));
+  CF* twf = reinterpret_cast<CF*>(xb + LINES * L::XBUF);
+  CI* twi = reinterpret_cast<CI*>(twf + L::N);
+  if constexpr (L::kFft) {
+    for (int i = threadIdx.x; i < L::N; i += blockDim.x) {
+      double s, c;
+      const int k1 = i / L::R2, t = i % L::R2;
+      sincospi(-2.0 * double((t * k1) % L::N) / L::N, &s, &c);
+      twf[i] = make_c<CF>(c, s);
+      const int nn = i / L::R1, k2 = i % L::R1;
+      sincospi(2.0 * double((nn * k2) % L::N) / L::N, &s, &c);
+      twi[i] = make_c<CI>(c, s);
+    }
   }
   __syncthreads();
   const int tid = threadIdx.x;
@@ -259,35 +264,59 @@ __global__ void __launch_bounds__(LINES * L::R2) line_pass_kernel(float2* __rest
 #pragma unroll
   for (int j = 0; j < L::R1; ++j) {
     const int e = t + L::R2 * j;
-    v[j] = axis == 0 ? f[(size_t)line * L::N + e] : f[(size_t)e * L::N + line];
+    v[j] = make_float2(0.f, 0.f);
+    if (line < n && e < n) v[j] = axis == 0 ? f[(size_t)line * n + e] : f[(size_t)e * n + line];
   }
-  L::propagate(v, t, q, xa + line_local * L::XBUF, xb + line_local * L::XBUF, twf, twi);
+  L::propagate(v, t, q, n, xa + line_local * L::XBUF, xb + line_local * L::XBUF, twf, twi);
 #pragma unroll
   for (int j = 0; j < L::R1; ++j) {
     const int e = t + L::R2 * j;
-    if (axis == 0) f[(size_t)line * L::N + e] = v[j];
-    else f[(size_t)e * L::N + line] = v[j];
+    if (line >= n || e >= n) continue;
+    if (axis == 0) f[(size_t)line * n + e] = v[j];
+    else f[(size_t)e * n + line] = v[j];
   }
 }
 
 template <class L, int LINES>
-int line_pass(float2* f, int axis, const float2* q, cudaStream_t s) {
-  const size_t smem = (2 * (size_t)LINES * L::XBUF + 2 * L::N) * sizeof(float2);
+int line_pass(int n, float2* f, int axis, const float2* q, cudaStream_t s) {
+  const size_t smem = 2 * (size_t)LINES * L::XBUF * sizeof(float2) + L::kTwiddleBytes;
   MM_CHECK_CUDA(cudaFuncSetAttribute(line_pass_kernel<L, LINES>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
                 "cudaFuncSetAttribute(line_pass)");
-  line_pass_kernel<L, LINES><<<L::N / LINES, LINES * L::R2, smem, s>>>(f, axis, q);
+  line_pass_kernel<L, LINES><<<(n + LINES - 1) / LINES, LINES * L::R2, smem, s>>>(f, n, axis, q);
   MM_CHECK_LAUNCH("line pass");
   return MM_OK;
 }
 
+bool fft_size(int n) { return n == 64 || n == 128 || n == 256 || n == 512; }
+
 int line_pass_any(int n, float2* f, int axis, const float2* q, cudaStream_t s) {
   switch (n) {
-    case 64: return line_pass<FftLine<8, 8>, 32>(f, axis, q, s);
-    case 128: return line_pass<FftLine<16, 8>, 32>(f, axis, q, s);
-    case 256: return line_pass<FftLine<16, 16>, 16>(f, axis, q, s);
-    case 512: return line_pass<FftLine<32, 16>, 8>(f, axis, q, s);
-    default: set_error("no FFT kernel for window %d", n); return MM_ERR_UNSUPPORTED;
+    case 64: return line_pass<FftLine<8, 8, double2>, 32>(n, f, axis, q, s);
+    case 128: return line_pass<FftLine<16, 8, double2>, 32>(n, f, axis, q, s);
+    case 256: return line_pass<FftLine<16, 16, double2>, 16>(n, f, axis, q, s);
+    case 512: return line_pass<FftLine<32, 16, double2>, 8>(n, f, axis, q, s);
+    default:
+      if (n <= 128) return line_pass<DenseLine<8>, 16>(n, f, axis, q, s);
+      return line_pass<DenseLine<32>, 16>(n, f, axis, q, s);
   }
+}
+
+// Circulant kernel of the scaled step for dense lines: p[m] = IDFT(Q)[m] (FP64).
+__global__ void base_p_kernel(float2* p, int n, double lam, double dz, double dx, double sc) {
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= n) return;
+  double re = 0.0, im = 0.0;
+  for (int k = 0; k < n; ++k) {
+    const int ks = k < n / 2 ? k : k - n;
+    const double f = ks / (n * dx);
+    double s, c;
+    sincos(-M_PI * lam * dz * f * f / sc, &s, &c);
+    double ws, wc;
+    sincospi(2.0 * double((long long)k * m % n) / n, &ws, &wc);
+    re += c * wc - s * ws;
+    im += c * ws + s * wc;
+  }
+  p[m] = make_float2(float(re / n), float(im / n));
 }
 
 // Transfer function of the scaled step along one axis, FFT order, 1/n folded.
@@ -387,7 +416,7 @@ extern "C" int mm_base_field(const mm_base_desc* desc, const void* pupil, void* 
                              void* stream) {
   MM_CHECK_ARG(desc && pupil && out && work && scratch && desc->edge1d, "NULL pointer");
   const int n = desc->n;
-  MM_CHECK_ARG(n == 64 || n == 128 || n == 256 || n == 512, "base field needs n in {64,128,256,512} (got %d)", n);
+  MM_CHECK_ARG(n >= 2 && n <= 512 && n % 2 == 0, "base field needs an even n <= 512 (got %d)", n);
   MM_CHECK_ARG(desc->dz > 0 && desc->d1 > 0 && desc->d2 > 0, "bad base-field geometry");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const double lam = desc->lambda_medium;
@@ -399,8 +428,9 @@ extern "C" int mm_base_field(const mm_base_desc* desc, const void* pupil, void* 
   float2* q = reinterpret_cast<float2*>(scratch + 256);
   MM_CHECK_ARG(n <= 1536, "scratch too small");
   const int blocks = std::min(256, (n * n + 255) / 256);
-  base_q_kernel<<<(n + 127) / 128, 128, 0, s>>>(q, n, lam, desc->dz, desc->d1, sc);
-  MM_CHECK_LAUNCH("base q");
+  if (fft_size(n)) base_q_kernel<<<(n + 127) / 128, 128, 0, s>>>(q, n, lam, desc->dz, desc->d1, sc);
+  else base_p_kernel<<<(n + 127) / 128, 128, 0, s>>>(q, n, lam, desc->dz, desc->d1, sc);
+  MM_CHECK_LAUNCH("base transfer function");
   base_pre_kernel<<<blocks, 256, 0, s>>>(static_cast<const float2*>(pupil), desc->edge1d, n, desc->d1, k, sc, desc->dz, v);
   MM_CHECK_LAUNCH("base pre-chirp");
   if (int rc = line_pass_any(n, v, 0, q, s)) return rc;

@@ -58,6 +58,7 @@ struct Params {
   long long total_items;
   // batched schedule: the stage / segment and first site of this launch
   int b_stage, b_k, b_site0;
+  int precision;  // MM_PRECISION_*: arithmetic of the radix-2 line transforms
 };
 
 constexpr long long kSpinLimit = 1ll << 24;  // ~ seconds with the backoff below
@@ -102,37 +103,89 @@ __device__ __forceinline__ float block_sum(float v, float* red) {
 
 // Twiddle tables for an N = R1*R2 line, in FP64 rounded once to float.
 template <class L>
-__device__ void fill_twiddles(float2* twf, float2* twi) {
+__device__ void fill_twiddles(typename L::CF* twf, typename L::CI* twi) {
+  if constexpr (!L::kFft) return;
   for (int i = threadIdx.x; i < L::N; i += blockDim.x) {
     {  // twf[k1*R2 + t] = exp(-2 pi i t k1 / N)
       const int k1 = i / L::R2, t = i % L::R2;
       double s, c;
       sincospi(-2.0 * double((t * k1) % L::N) / L::N, &s, &c);
-      twf[i] = make_float2(float(c), float(s));
+      twf[i] = make_c<typename L::CF>(c, s);
     }
     {  // twi[n*R1 + k1] = exp(+2 pi i n k1 / N)
       const int nn = i / L::R1, k1 = i % L::R1;
       double s, c;
       sincospi(2.0 * double((nn * k1) % L::N) / L::N, &s, &c);
-      twi[i] = make_float2(float(c), float(s));
+      twi[i] = make_c<typename L::CI>(c, s);
     }
   }
 }
 
+// Which line of the item this thread works on, and its place in the line:
+// rows (axis 0) keep a line's threads in one warp; columns (axis 1) put 32
+// consecutive columns in a warp so every global access is a full segment.
+template <class L, int LINES>
+struct Lane {
+  int axis, line_local, t, line;
+  __device__ Lane(const Params& p, const Item& it) {
+    const StageP& st = p.st[it.stage];
+    axis = (st.seg0 + it.k) & 1;
+    const int tid = threadIdx.x;
+    line_local = axis == 0 ? tid / L::R2 : tid % LINES;
+    t = axis == 0 ? tid % L::R2 : tid / LINES;
+    line = it.block * LINES + line_local;
+  }
+};
+
+// Window offset of the item's site; an offset outside the screen volume is
+// flagged (reported as MM_ERR_ARGUMENT) and replaced by the volume's corner.
+__device__ __forceinline__ int2 site_offset(const Params& p, const Item& it) {
+  const StageP& st = p.st[it.stage];
+  int xo = __ldg(p.offsets + 2 * it.site), yo = __ldg(p.offsets + 2 * it.site + 1);
+  if (xo < 0 || yo < 0 || xo + st.size > st.vol_h || yo + st.size > st.vol_w) {
+    if (threadIdx.x == 0) atomicOr(p.error, 2);
+    xo = 0;
+    yo = 0;
+  }
+  return make_int2(xo, yo);
+}
+
+// Start the asynchronous copy of this thread's screen samples into shared
+// memory (slot j*blockDim + tid); they are consumed after the first half step.
+template <class L, int LINES>
+__device__ void prefetch_screen(const Params& p, const Item& it, float2* scr_s) {
+  const StageP& st = p.st[it.stage];
+  if (it.k >= st.steps) return;
+  const Lane<L, LINES> ln(p, it);
+  const int N = st.size;
+  const int2 o = site_offset(p, it);
+  const float2* scr = st.screens + (size_t)it.k * st.vol_h * st.vol_w;
+#pragma unroll
+  for (int j = 0; j < L::R1; ++j) {
+    const int e = ln.t + L::R2 * j;
+    if (!(L::kFft || (ln.line < N && e < N))) continue;
+    const int row = ln.axis == 0 ? ln.line : e;
+    const int col = ln.axis == 0 ? e : ln.line;
+    cp_async8(scr_s + j * blockDim.x + threadIdx.x, scr + (size_t)(o.x + row) * st.vol_w + (o.y + col));
+  }
+  cp_async_commit();
+}
+
 // One (site, segment, line block) work item.
 template <class L, int LINES>
-__device__ void process(const Params& p, const Item& it, float2* xa, float2* xb, const float2* twf,
-                        const float2* twi, float* red) {
+__device__ void process(const Params& p, const Item& it, float2* xa, float2* xb, const typename L::CF* twf,
+                        const typename L::CI* twi, float* red, const float2* scr_s) {
   constexpr int R1 = L::R1, R2 = L::R2;
   const StageP& st = p.st[it.stage];
   const int N = st.size;
-  const int axis = (st.seg0 + it.k) & 1;  // 0: lines are rows, 1: lines are columns
-  const int tid = threadIdx.x;
-  const int line_local = axis == 0 ? tid / R2 : tid % LINES;
-  const int t = axis == 0 ? tid % R2 : tid / LINES;
-  const int line = it.block * LINES + line_local;
+  const Lane<L, LINES> ln(p, it);
+  const int axis = ln.axis, line_local = ln.line_local, t = ln.t, line = ln.line;
   float2* xa_l = xa + line_local * L::XBUF;
   float2* xb_l = xb + line_local * L::XBUF;
+  // Radix-2 lines exactly fill their threads; the dense policy guards lines
+  // and samples beyond the window (those threads still take every barrier).
+  const bool live = L::kFft || line < N;
+  auto in_line = [&](int e) { return L::kFft || (live && e < N); };
 
   float2 v[R1];
   // ------------------------------------------------------------------ load
@@ -144,8 +197,9 @@ __device__ void process(const Params& p, const Item& it, float2* xa, float2* xb,
       const int e = t + R2 * j;
       const int row = axis == 0 ? line : e;
       const int col = axis == 0 ? e : line;
-      float2 a;
-      if (it.k > 0) {
+      float2 a = make_float2(0.f, 0.f);
+      if (!in_line(e)) {
+      } else if (it.k > 0) {
         const float2* buf = (it.stage == 1) ? p.bufB + slot_b : p.bufA + slot_a;
         a = __ldcg(buf + (size_t)row * N + col);
       } else if (it.stage == 0) {
@@ -162,26 +216,17 @@ __device__ void process(const Params& p, const Item& it, float2* xa, float2* xb,
     }
   }
   // ---------------------------------------- second half of step k-1
-  if (it.k > 0) L::propagate(v, t, st.kern + (size_t)(it.k - 1) * N, xa_l, xb_l, twf, twi);
+  if (it.k > 0) L::propagate(v, t, st.kern + (size_t)(it.k - 1) * N, N, xa_l, xb_l, twf, twi);
   // ------------------------------------------------------- screen of step k
   if (it.k < st.steps) {
-    const float2* scr = st.screens + (size_t)it.k * st.vol_h * st.vol_w;
-    int xo = __ldg(p.offsets + 2 * it.site), yo = __ldg(p.offsets + 2 * it.site + 1);
-    if (xo < 0 || yo < 0 || xo + N > st.vol_h || yo + N > st.vol_w) {
-      // A window outside the screen volume: flag it (the host reports
-      // MM_ERR_ARGUMENT) and read the volume's corner instead of out of bounds.
-      if (threadIdx.x == 0) atomicOr(p.error, 2);
-      xo = 0;
-      yo = 0;
-    }
-    const float eline = __ldg(st.edge + line);
+    const float eline = live ? __ldg(st.edge + line) : 0.f;
+    cp_async_wait_all();
 #pragma unroll
     for (int j = 0; j < R1; ++j) {
       const int e = t + R2 * j;
-      const int row = axis == 0 ? line : e;
-      const int col = axis == 0 ? e : line;
+      if (!in_line(e)) continue;
       const float w = axis == 0 ? eline * __ldg(st.edge + e) : __ldg(st.edge + e) * eline;
-      float2 s = __ldg(scr + (size_t)(xo + row) * st.vol_w + (yo + col));
+      float2 s = scr_s[j * blockDim.x + threadIdx.x];
       s = make_float2(s.x * w, s.y * w);
       v[j] = cmul(v[j], s);
     }
@@ -201,7 +246,7 @@ __device__ void process(const Params& p, const Item& it, float2* xa, float2* xb,
         const int e = t + R2 * j;
         const int r2 = (axis == 0 ? line : e) - p.crop0;
         const int c2 = (axis == 0 ? e : line) - p.crop0;
-        if (r2 >= 0 && r2 < p.n2 && c2 >= 0 && c2 < p.n2) {
+        if (in_line(e) && r2 >= 0 && r2 < p.n2 && c2 >= 0 && c2 < p.n2) {
           const float pw = photon_power(v[j], p.order);
           psum += pw;
           float* dst = img + (size_t)r2 * p.n2 + c2;
@@ -218,18 +263,19 @@ __device__ void process(const Params& p, const Item& it, float2* xa, float2* xb,
         const int e = t + R2 * j;
         const int r = (axis == 0 ? line : e) - p.fx0;
         const int c = (axis == 0 ? e : line) - p.fy0;
-        if (r >= 0 && r < p.fh && c >= 0 && c < p.fw) __stcs(dst + (size_t)r * p.fw + c, photon_power(v[j], p.order));
+        if (in_line(e) && r >= 0 && r < p.fh && c >= 0 && c < p.fw) __stcs(dst + (size_t)r * p.fw + c, photon_power(v[j], p.order));
       }
     }
   }
   // ---------------------------------------- first half of step k
-  if (it.k < st.steps) L::propagate(v, t, st.kern + (size_t)it.k * N, xa_l, xb_l, twf, twi);
+  if (it.k < st.steps) L::propagate(v, t, st.kern + (size_t)it.k * N, N, xa_l, xb_l, twf, twi);
   // ------------------------------------------------------------------ store
   if (!(it.stage == 2 && it.k == st.steps)) {
     float2* buf = (it.stage == 1) ? p.bufB + (size_t)it.slot * p.n2 * p.n2 : p.bufA + (size_t)it.slot * p.n * p.n;
 #pragma unroll
     for (int j = 0; j < R1; ++j) {
       const int e = t + R2 * j;
+      if (!in_line(e)) continue;
       const int row = axis == 0 ? line : e;
       const int col = axis == 0 ? e : line;
       __stcg(buf + (size_t)row * N + col, v[j]);
@@ -239,18 +285,21 @@ __device__ void process(const Params& p, const Item& it, float2* xa, float2* xb,
 
 template <class L, int LINES>
 struct Smem {
-  static constexpr size_t xbuf = (size_t)LINES * L::XBUF;
-  static constexpr size_t bytes = (2 * xbuf + 2 * L::N) * sizeof(float2) + 32 * sizeof(float);
+  static constexpr size_t xbuf = (size_t)LINES * L::XBUF;     // float2 per exchange buffer (even count)
+  static constexpr size_t screen = (size_t)LINES * L::R2 * L::R1;  // float2: one screen tile
+  static constexpr size_t bytes =
+      2 * xbuf * sizeof(float2) + L::kTwiddleBytes + screen * sizeof(float2) + 32 * sizeof(float);
 };
 
 template <class L, int LINES>
-__global__ void __launch_bounds__(LINES * L::R2) persistent_kernel(Params p) {
+__global__ void __launch_bounds__(LINES * L::R2, 2) persistent_kernel(Params p) {
   extern __shared__ float4 smem_raw[];
   float2* xa = reinterpret_cast<float2*>(smem_raw);
   float2* xb = xa + Smem<L, LINES>::xbuf;
-  float2* twf = xb + Smem<L, LINES>::xbuf;
-  float2* twi = twf + L::N;
-  float* red = reinterpret_cast<float*>(twi + L::N);
+  auto* twf = reinterpret_cast<typename L::CF*>(xb + Smem<L, LINES>::xbuf);
+  auto* twi = reinterpret_cast<typename L::CI*>(reinterpret_cast<char*>(twf) + (L::kFft ? L::N * sizeof(typename L::CF) : 0));
+  float2* scr_s = reinterpret_cast<float2*>(reinterpret_cast<char*>(twi) + (L::kFft ? L::N * sizeof(typename L::CI) : 0));
+  float* red = reinterpret_cast<float*>(scr_s + Smem<L, LINES>::screen);
   __shared__ long long s_item;
   __shared__ int s_abort;
   fill_twiddles<L>(twf, twi);
@@ -263,6 +312,7 @@ __global__ void __launch_bounds__(LINES * L::R2) persistent_kernel(Params p) {
     Item it;
     const bool live = decode(p, item, it);
     if (live) {
+      prefetch_screen<L, LINES>(p, it, scr_s);  // inputs only: safe before the dependency wait
       if (threadIdx.x == 0) {
         const StageP& st = p.st[it.stage];
         const unsigned need = unsigned(it.wave * p.blocks_per_site + st.cum0 + (long long)it.k * st.nblocks);
@@ -282,7 +332,7 @@ __global__ void __launch_bounds__(LINES * L::R2) persistent_kernel(Params p) {
       }
       __syncthreads();
       if (s_abort) break;
-      process<L, LINES>(p, it, xa, xb, twf, twi, red);
+      process<L, LINES>(p, it, xa, xb, twf, twi, red, scr_s);
       __syncthreads();
       if (threadIdx.x == 0) {
         __threadfence();
@@ -294,13 +344,14 @@ __global__ void __launch_bounds__(LINES * L::R2) persistent_kernel(Params p) {
 }
 
 template <class L, int LINES>
-__global__ void __launch_bounds__(LINES * L::R2) batched_kernel(Params p) {
+__global__ void __launch_bounds__(LINES * L::R2, 2) batched_kernel(Params p) {
   extern __shared__ float4 smem_raw[];
   float2* xa = reinterpret_cast<float2*>(smem_raw);
   float2* xb = xa + Smem<L, LINES>::xbuf;
-  float2* twf = xb + Smem<L, LINES>::xbuf;
-  float2* twi = twf + L::N;
-  float* red = reinterpret_cast<float*>(twi + L::N);
+  auto* twf = reinterpret_cast<typename L::CF*>(xb + Smem<L, LINES>::xbuf);
+  auto* twi = reinterpret_cast<typename L::CI*>(reinterpret_cast<char*>(twf) + (L::kFft ? L::N * sizeof(typename L::CF) : 0));
+  float2* scr_s = reinterpret_cast<float2*>(reinterpret_cast<char*>(twi) + (L::kFft ? L::N * sizeof(typename L::CI) : 0));
+  float* red = reinterpret_cast<float*>(scr_s + Smem<L, LINES>::screen);
   fill_twiddles<L>(twf, twi);
   __syncthreads();
   const StageP& st = p.st[p.b_stage];
@@ -312,7 +363,8 @@ __global__ void __launch_bounds__(LINES * L::R2) batched_kernel(Params p) {
   it.site = p.b_site0 + it.slot;
   it.wave = 0;
   if (it.site >= p.nsites) return;
-  process<L, LINES>(p, it, xa, xb, twf, twi, red);
+  prefetch_screen<L, LINES>(p, it, scr_s);
+  process<L, LINES>(p, it, xa, xb, twf, twi, red, scr_s);
 }
 
 // ------------------------------------------------------------------- host --
@@ -320,13 +372,21 @@ struct Config {
   int r1, r2, lines;
 };
 
+bool fft_size(int n) { return n == 64 || n == 128 || n == 256 || n == 512; }
+
+// Lines per CTA for a window; dense windows use 16 lines of 16 threads.
 bool line_config(int n, Config& c) {
   switch (n) {
     case 64: c = {8, 8, 32}; return true;
     case 128: c = {16, 8, 32}; return true;
     case 256: c = {16, 16, 16}; return true;
     case 512: c = {32, 16, 8}; return true;
-    default: return false;
+    default:
+      if (n >= 2 && n <= 512 && n % 2 == 0) {
+        c = {n <= 128 ? 8 : 32, 16, 16};
+        return true;
+      }
+      return false;
   }
 }
 
@@ -373,13 +433,29 @@ int launch_batched(Params& p, int stage, int k, int site0, int batch, cudaStream
   return MM_OK;
 }
 
-int launch_batched_any(Params& p, int stage, int k, int site0, int batch, cudaStream_t s) {
+template <class CF, class CI>
+int launch_batched_fft(Params& p, int stage, int k, int site0, int batch, cudaStream_t s) {
   switch (p.st[stage].size) {
-    case 64: return launch_batched<FftLine<8, 8>, 32>(p, stage, k, site0, batch, s);
-    case 128: return launch_batched<FftLine<16, 8>, 32>(p, stage, k, site0, batch, s);
-    case 256: return launch_batched<FftLine<16, 16>, 16>(p, stage, k, site0, batch, s);
-    case 512: return launch_batched<FftLine<32, 16>, 8>(p, stage, k, site0, batch, s);
-    default: set_error("no propagation kernel for window %d", p.st[stage].size); return MM_ERR_UNSUPPORTED;
+    case 64: return launch_batched<FftLine<8, 8, CF, CI>, 32>(p, stage, k, site0, batch, s);
+    case 128: return launch_batched<FftLine<16, 8, CF, CI>, 32>(p, stage, k, site0, batch, s);
+    case 256: return launch_batched<FftLine<16, 16, CF, CI>, 16>(p, stage, k, site0, batch, s);
+    default: return launch_batched<FftLine<32, 16, CF, CI>, 8>(p, stage, k, site0, batch, s);
+  }
+}
+
+int launch_batched_any(Params& p, int stage, int k, int site0, int batch, cudaStream_t s) {
+  const int n = p.st[stage].size;
+  switch (n) {
+    case 64:
+    case 128:
+    case 256:
+    case 512:
+      if (p.precision == MM_PRECISION_FP64) return launch_batched_fft<double2, double2>(p, stage, k, site0, batch, s);
+      if (p.precision == MM_PRECISION_MIXED) return launch_batched_fft<float2, double2>(p, stage, k, site0, batch, s);
+      return launch_batched_fft<float2, float2>(p, stage, k, site0, batch, s);
+    default:
+      if (n <= 128) return launch_batched<DenseLine<8>, 16>(p, stage, k, site0, batch, s);
+      return launch_batched<DenseLine<32>, 16>(p, stage, k, site0, batch, s);
   }
 }
 
@@ -403,14 +479,24 @@ int launch_persistent(Params& p, cudaStream_t s) {
   return MM_OK;
 }
 
-int launch_persistent_any(Params& p, cudaStream_t s) {
+template <class CF, class CI>
+int launch_persistent_fft(Params& p, cudaStream_t s) {
   switch (p.n) {
-    case 64: return launch_persistent<FftLine<8, 8>, 32>(p, s);
-    case 128: return launch_persistent<FftLine<16, 8>, 32>(p, s);
-    case 256: return launch_persistent<FftLine<16, 16>, 16>(p, s);
-    case 512: return launch_persistent<FftLine<32, 16>, 8>(p, s);
-    default: set_error("no propagation kernel for window %d", p.n); return MM_ERR_UNSUPPORTED;
+    case 64: return launch_persistent<FftLine<8, 8, CF, CI>, 32>(p, s);
+    case 128: return launch_persistent<FftLine<16, 8, CF, CI>, 32>(p, s);
+    case 256: return launch_persistent<FftLine<16, 16, CF, CI>, 16>(p, s);
+    default: return launch_persistent<FftLine<32, 16, CF, CI>, 8>(p, s);
   }
+}
+
+int launch_persistent_any(Params& p, cudaStream_t s) {
+  if (!fft_size(p.n) || p.n != p.n2) {
+    if (std::max(p.n, p.n2) <= 128) return launch_persistent<DenseLine<8>, 16>(p, s);
+    return launch_persistent<DenseLine<32>, 16>(p, s);
+  }
+  if (p.precision == MM_PRECISION_FP64) return launch_persistent_fft<double2, double2>(p, s);
+  if (p.precision == MM_PRECISION_MIXED) return launch_persistent_fft<float2, double2>(p, s);
+  return launch_persistent_fft<float2, float2>(p, s);
 }
 
 int build_params(const mm_stage_plan* plan, int slots, Params& p) {
@@ -431,7 +517,7 @@ int build_params(const mm_stage_plan* plan, int slots, Params& p) {
     Config c;
     MM_CHECK_ARG(d.size == (s == 1 ? plan->n2 : plan->n), "stage %d window %d does not match the plan", s, d.size);
     if (!line_config(d.size, c)) {
-      set_error("no propagation kernel for window %d (supported: 64, 128, 256, 512)", d.size);
+      set_error("no propagation kernel for window %d (even sizes up to 512)", d.size);
       return MM_ERR_UNSUPPORTED;
     }
     MM_CHECK_ARG(d.steps >= 1 && d.screens && d.edge1d && d.kernels, "stage %d incomplete", s);
@@ -440,7 +526,7 @@ int build_params(const mm_stage_plan* plan, int slots, Params& p) {
     st.size = d.size;
     st.steps = d.steps;
     st.nseg = d.steps + 1;
-    st.nblocks = d.size / c.lines;
+    st.nblocks = (d.size + c.lines - 1) / c.lines;
     st.screens = static_cast<const float2*>(d.screens);
     st.vol_h = d.vol_h;
     st.vol_w = d.vol_w;
@@ -478,6 +564,10 @@ int build_params(const mm_stage_plan* plan, int slots, Params& p) {
   p.offsets = plan->offsets;
   p.nsites = plan->nsites;
   p.slots = slots;
+  MM_CHECK_ARG(plan->precision == MM_PRECISION_FP32 || plan->precision == MM_PRECISION_FP64 ||
+                   plan->precision == MM_PRECISION_MIXED,
+               "unknown precision %d", plan->precision);
+  p.precision = plan->precision;
   p.blocks_per_site = cum;
   return MM_OK;
 }
@@ -521,7 +611,8 @@ extern "C" int mm_propagate_sites(const mm_stage_plan* plan, int schedule, int s
                 "zero queue state");
   int rc = MM_OK;
   if (schedule == MM_SCHEDULE_PERSISTENT) {
-    MM_CHECK_ARG(plan->n == plan->n2, "the persistent schedule needs n == n2 (got %d, %d); use the batched one",
+    MM_CHECK_ARG(plan->n == plan->n2 || !(fft_size(plan->n) && fft_size(plan->n2)),
+                 "the persistent schedule needs one kernel for both windows (got %d, %d); use the batched one",
                  plan->n, plan->n2);
     const int waves = (plan->nsites + slots - 1) / slots;
     p.total_items = (long long)waves * slots * p.blocks_per_site;

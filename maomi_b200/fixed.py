@@ -108,27 +108,28 @@ def assemble(config, out, shape, *, mask_mode="matlab_v4", z_positions=None, cut
     return result
 
 
-def run_stage(config, raw_fields, points_um=None, *, uin=None, device="cuda", tails=True, count_per_axis=65,
-              slots=64, schedule=None, return_psf_3d=True, plan=None, timings=None, check=True):
-    """Fused optical stage: every product reduced on the device.
+def stage_device(config, raw_fields, points_um=None, *, uin=None, device="cuda", tails=True, count_per_axis=65,
+                 slots=64, schedule=None, plan=None, check=True, events=None, precision="fp64"):
+    """Fused optical stage leaving every product on the device.
 
-    Returns the dictionary of ``assemble`` / maomi.optics.propagate with FP64
-    energies, v4 masks and site-averaged tails.  ``plan`` reuses an existing
-    ``OpticalPlan``; ``timings`` (a dict) receives per-phase seconds."""
+    Phase preparation (inside ``OpticalPlan``), the persistent propagation of
+    every site with both tails reduced on the fly, focal PSF finalisation with
+    FP64 site sums and the FP64 v4 mask assembly.  Returns a dict of device
+    tensors (``psf_3d``, ``energies``, ``psf_sum``, ``psf_abs_sum``, ``masks``,
+    tail ``profiles``/``weights``/``convmask``) plus the plan.  ``events``
+    (a pair of CUDA events) brackets the propagation launch."""
     import torch
     from .backends.cuda.batched import OpticalPlan, trapezoid
     _lib.require_cuda(device)
-    t0 = time.perf_counter()
     if plan is None:
-        plan = OpticalPlan(config, raw_fields, uin=uin, device=device)
+        plan = OpticalPlan(config, raw_fields, uin=uin, device=device, precision=precision)
     points = fixed_locations(config, count_per_axis) if points_um is None else np.asarray(points_um, float)
     pts, off = plan.offsets(points)
     P = len(pts)
+    dev = plan.device
     with torch.inference_mode():
-        res = plan.run_sites(off, tail_per_site=False, slots=slots, schedule=schedule, check=check)
+        res = plan.run_sites(off, tail_per_site=False, slots=slots, schedule=schedule, check=check, events=events)
         psf, energies, s1, s2 = plan.finalize_focal(res["focal"], psf=True, sums=True)
-        dev = plan.device
-        r = config.vres
         prof, wts = [], []
         for j in range(2):
             axial = plan.axial["top" if j == 0 else "bottom"].astype(np.float64)
@@ -136,9 +137,9 @@ def run_stage(config, raw_fields, points_um=None, *, uin=None, device="cuda", ta
             prof.append(pj)
             wts.append((pj * torch.as_tensor(trapezoid(len(axial)), device=dev)).sum(1) * config.prop_um)
         values = torch.stack([energies, wts[0], wts[1]] if tails else [energies], 1)
-        shape = tuple(np.round(np.array(config.volume_um[:2]) * r).astype(int))
-        p_dev, coef = v4_coefficients_device(pts * r, values, device=dev) if P > 1 else (None, None)
+        shape = tuple(int(v) for v in np.round(np.array(config.volume_um[:2]) * config.vres))
         if P > 1:
+            p_dev, coef = v4_coefficients_device(pts * config.vres, values, device=dev)
             masks = v4_evaluate_grid_device(p_dev, coef, *shape, device=dev)
         else:
             masks = values[0].reshape(1, 1, -1).expand(shape[0], shape[1], -1).contiguous()
@@ -154,40 +155,71 @@ def run_stage(config, raw_fields, points_um=None, *, uin=None, device="cuda", ta
                           _lib.ptr(rt.my), X, Y, float(config.ss ** 4) / P, _lib.ptr(conv), _lib.ptr(scratch),
                           _lib.stream_of(dev))
                 convs.append(conv)
-        # ---- host copies of the final products
-        masks_h = masks.cpu().numpy()
-        psf_abs = (s2 / P).cpu().numpy()
-        psf_raw = (s1 / P).cpu().numpy()
-        energies_h = energies.cpu().numpy()
-        psf_3d = psf.cpu().numpy() if return_psf_3d else None
-        prof_h = [p.cpu().numpy() for p in prof]
-        wts_h = [w.cpu().numpy() for w in wts]
-        convs_h = [c.cpu().numpy() for c in convs]
-        neg = float(-torch.clamp(psf, max=0).sum(dtype=torch.float64) / torch.clamp(s2.sum(), min=1e-30))
+    return dict(plan=plan, points_um=pts, psf_3d=psf, energies=energies, psf_sum=s1, psf_abs_sum=s2, masks=masks,
+                profiles=prof, weights=wts, convmask=convs, tails=bool(tails))
+
+
+def stage_to_host(config, dev, *, return_psf_3d=True, out=None):
+    """Host result dictionary (the keys of maomi.optics.propagate / assemble)
+    from ``stage_device`` output.  ``out`` may hold pinned host buffers."""
+    import torch
+    plan, P = dev["plan"], len(dev["points_um"])
+
+    def host(t, key):
+        if out is not None and key in out:
+            out[key].copy_(t, non_blocking=True)
+            return out[key]
+        return t.cpu()
+
+    with torch.inference_mode():
+        masks_h = host(dev["masks"], "masks")
+        psf_abs = host(dev["psf_abs_sum"] / P, "psf")
+        psf_raw = host(dev["psf_sum"] / P, "psf_raw")
+        energies = host(dev["energies"], "energies")
+        psf_3d = host(dev["psf_3d"], "psf_3d") if return_psf_3d else None
+        prof = [host(p, f"profile{j}") for j, p in enumerate(dev["profiles"])]
+        wts = [host(w, f"weight{j}") for j, w in enumerate(dev["weights"])]
+        convs = [host(c, f"convmask{j}") for j, c in enumerate(dev["convmask"])]
+        neg = -torch.clamp(dev["psf_3d"], max=0).sum(dtype=torch.float64) / torch.clamp(dev["psf_abs_sum"].sum(),
+                                                                                          min=1e-30)
+        neg = float(neg)
+    torch.cuda.current_stream(plan.device).synchronize()
+    masks_h = masks_h.numpy()
     mask = masks_h[..., 0]
     mean = float(mask.mean())
     if not np.isfinite(mean) or mean <= 0:
         raise ValueError("Nonpositive or invalid mean excitation energy")
     result = {
-        "psf": psf_abs, "psf_raw": psf_raw, "psf_3d": psf_3d, "points_um": pts, "energies": energies_h,
+        "psf": psf_abs.numpy(), "psf_raw": psf_raw.numpy(),
+        "psf_3d": psf_3d.numpy() if psf_3d is not None else None,
+        "points_um": dev["points_um"], "energies": energies.numpy(),
         "mask_raw": mask, "mask": mask / mean, "mask_mean": mean, "mask_mode": "matlab_v4",
-        "tails_computed": bool(tails), "unique_optical_paths": P,
+        "tails_computed": dev["tails"], "unique_optical_paths": P,
         "negative_resampling_mass_fraction": neg,
     }
-    if tails:
+    if dev["tails"]:
         for j, name in enumerate(("psfT", "psfB")):
             z = plan.z_positions[0][plan.cut:] if j == 0 else plan.z_positions[2]
             tm = masks_h[..., j + 1]
             tm_mean = float(tm.mean())
+            prof_j, wts_j = prof[j].numpy(), wts[j].numpy()
             result[name] = {
-                "convmask": convs_h[j], "weight": float(wts_h[j].mean()),
-                "psfZ": _psf_z(config, z, prof_h[j].sum(0)),
+                "convmask": convs[j].numpy(), "weight": float(wts_j.mean()),
+                "psfZ": _psf_z(config, z, prof_j.sum(0)),
                 "mask_raw": tm, "mask": tm / tm_mean if tm_mean > 0 else tm, "mask_mean": tm_mean,
-                "weights_per_point": wts_h[j], "profiles_per_point": prof_h[j],
+                "weights_per_point": wts_j, "profiles_per_point": prof_j,
             }
-    if timings is not None:
-        timings["stage"] = time.perf_counter() - t0
     return result
+
+
+def run_stage(config, raw_fields, points_um=None, *, uin=None, device="cuda", tails=True, count_per_axis=65,
+              slots=64, schedule=None, return_psf_3d=True, plan=None, check=True, precision="fp64"):
+    """The whole optical stage on the GPU, returning the host result dictionary
+    of maomi.optics.propagate (optics.py:341-381) / fixed.assemble."""
+    dev = stage_device(config, raw_fields, points_um, uin=uin, device=device, tails=tails,
+                       count_per_axis=count_per_axis, slots=slots, schedule=schedule, plan=plan, check=check,
+                       precision=precision)
+    return stage_to_host(config, dev, return_psf_3d=return_psf_3d)
 
 
 def run_fixed(config, volume=None, *, vessels=None, raw_fields=None, scatter=True, custom_phase=None,
