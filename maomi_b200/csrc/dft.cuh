@@ -197,7 +197,10 @@ struct FftLine {
   static constexpr int N = R1 * R2;
   static constexpr int J = R1 / R2;  // columns of the second pass per thread
   static constexpr int PITCH = R2 + 1;
-  static constexpr int XBUF = R1 * PITCH;  // float2 per line per buffer
+  // float2 per line per buffer: padded to 1 (mod 16) so consecutive lines
+  // start on consecutive 8-byte bank pairs; in the column layout a warp holds
+  // 16-32 different lines at the same in-line offset.
+  static constexpr int XBUF = (R1 * PITCH + 15) / 16 * 16 + 1;
   static constexpr bool kFft = true;
   static constexpr size_t kTwiddleBytes = (size_t)N * (sizeof(CF) + sizeof(CI));
   static_assert(R1 % R2 == 0, "R2 must divide R1");
@@ -264,7 +267,7 @@ struct DenseLine {
   static constexpr int R1 = RMAX;
   static constexpr int R2 = 16;
   static constexpr int N = RMAX * 16;  // capacity
-  static constexpr int XBUF = N;
+  static constexpr int XBUF = N + 1;  // odd stride: lines start on different banks
   static constexpr bool kFft = false;
 
   __device__ static void propagate(float2 (&v)[R1], int t, const float2* __restrict__ ker, int n, float2* xa,
