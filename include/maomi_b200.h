@@ -197,6 +197,19 @@ size_t mm_propagate_workspace_size(const mm_stage_plan* plan, int slots, int sch
 int mm_propagate_sites(const mm_stage_plan* plan, int schedule, int slots, void* workspace,
                        size_t workspace_bytes, int check, void* stream);
 
+/* Propagation for callers that cannot allocate device memory (no counterpart
+ * in the reference).  Same work and outputs as mm_propagate_sites, with the
+ * workspace taken from a fixed 32 MiB device array inside the library instead
+ * of a caller buffer: hosts that reserve the whole device heap for their own
+ * pool, or code that must not call cudaMalloc once running, can still
+ * propagate.  Plans needing more scratch than the array holds (at n = n2 = 256,
+ * more than 31 sites in flight) are rejected with MM_ERR_ARGUMENT.  The first
+ * call on a device looks up the array's address with that device current;
+ * make it before any stream capture.  All calls share the array (it keeps the
+ * last call's contents); calls that overlap on the GPU race, so serialise
+ * them.  Calls no cudaMalloc or cudaFree. */
+int mm_propagate_sites_noalloc(const mm_stage_plan* plan, int schedule, int slots, int check, void* stream);
+
 /* ------------------------------------------------------------------------
  * Focal PSF finalisation: psf[p,x,y,z] = scale*axial[z] *
  *   sum_i wx[x,i] sum_j wy[y,j] focal[p,z,ix[x,i],iy[y,j]]
