@@ -205,7 +205,10 @@ struct FftLine {
   static constexpr size_t kTwiddleBytes = (size_t)N * (sizeof(CF) + sizeof(CI));
   static_assert(R1 % R2 == 0, "R2 must divide R1");
 
-  // twf[k1*R2 + t] = W_N^(t*k1) (CF);  twi[n*R1 + k1] = W_N^(-n*k1) (CI)
+  // twf[k1*R2 + t] = W_N^(t*k1) (CF);  twi[n*R1 + k1] = W_N^(-n*k1) (CI).
+  // SINGLE: xa and xb are the same buffer; two more barriers keep the
+  // exchanges apart (and the next call's first exchange after this one's last).
+  template <bool SINGLE = false>
   __device__ static void propagate(float2 (&x)[R1], int t, const float2* __restrict__ q, int /*n*/,
                                    float2* xa, float2* xb, const CF* twf, const CI* twi) {
     CF v[R1];
@@ -235,6 +238,7 @@ struct FftLine {
     // ---- inverse pass 1: IDFT over k2 -> n_a, twiddle W_N^(-n_a*k1), exchange
 #pragma unroll
     for (int j = 0; j < J; ++j) dft<R2, +1>(w + j * R2);
+    if constexpr (SINGLE) __syncthreads();  // forward reads of the shared buffer done
 #pragma unroll
     for (int j = 0; j < J; ++j)
 #pragma unroll
@@ -251,6 +255,7 @@ struct FftLine {
     dft<R1, +1>(w);
 #pragma unroll
     for (int m = 0; m < R1; ++m) x[m] = to_f2(w[m]);
+    if constexpr (SINGLE) __syncthreads();  // inverse reads done before the buffer is reused
   }
 };
 
@@ -270,6 +275,7 @@ struct DenseLine {
   static constexpr int XBUF = N + 1;  // odd stride: lines start on different banks
   static constexpr bool kFft = false;
 
+  template <bool SINGLE = false>
   __device__ static void propagate(float2 (&v)[R1], int t, const float2* __restrict__ ker, int n, float2* xa,
                                    float2* /*xb*/, const CF* /*twf*/, const CI* /*twi*/) {
 #pragma unroll

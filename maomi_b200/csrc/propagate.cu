@@ -63,6 +63,9 @@ struct Params {
 
 constexpr long long kSpinLimit = 1ll << 24;  // ~ seconds with the backoff below
 
+// Lines per CTA (128 threads each: four CTAs, 16 warps, per SM).
+constexpr int kLines64 = 16, kLines128 = 16, kLines256 = 8, kLines512 = 8, kLinesDense = 8;
+
 struct Item {
   int stage, k, slot, block, site, wave;
 };
@@ -181,7 +184,7 @@ __device__ void process(const Params& p, const Item& it, float2* xa, float2* xb,
   const Lane<L, LINES> ln(p, it);
   const int axis = ln.axis, line_local = ln.line_local, t = ln.t, line = ln.line;
   float2* xa_l = xa + line_local * L::XBUF;
-  float2* xb_l = xb + line_local * L::XBUF;
+  float2* xb_l = xa_l;  // one exchange buffer per line (see propagate<SINGLE>)
   // Radix-2 lines exactly fill their threads; the dense policy guards lines
   // and samples beyond the window (those threads still take every barrier).
   const bool live = L::kFft || line < N;
@@ -216,7 +219,7 @@ __device__ void process(const Params& p, const Item& it, float2* xa, float2* xb,
     }
   }
   // ---------------------------------------- second half of step k-1
-  if (it.k > 0) L::propagate(v, t, st.kern + (size_t)(it.k - 1) * N, N, xa_l, xb_l, twf, twi);
+  if (it.k > 0) L::template propagate<true>(v, t, st.kern + (size_t)(it.k - 1) * N, N, xa_l, xb_l, twf, twi);
   // ------------------------------------------------------- screen of step k
   if (it.k < st.steps) {
     const float eline = live ? __ldg(st.edge + line) : 0.f;
@@ -268,7 +271,7 @@ __device__ void process(const Params& p, const Item& it, float2* xa, float2* xb,
     }
   }
   // ---------------------------------------- first half of step k
-  if (it.k < st.steps) L::propagate(v, t, st.kern + (size_t)it.k * N, N, xa_l, xb_l, twf, twi);
+  if (it.k < st.steps) L::template propagate<true>(v, t, st.kern + (size_t)it.k * N, N, xa_l, xb_l, twf, twi);
   // ------------------------------------------------------------------ store
   if (!(it.stage == 2 && it.k == st.steps)) {
     float2* buf = (it.stage == 1) ? p.bufB + (size_t)it.slot * p.n2 * p.n2 : p.bufA + (size_t)it.slot * p.n * p.n;
@@ -288,27 +291,30 @@ struct Smem {
   static constexpr size_t xbuf = (size_t)LINES * L::XBUF;     // float2 per exchange buffer (even count)
   static constexpr size_t screen = (size_t)LINES * L::R2 * L::R1;  // float2: one screen tile
   static constexpr size_t bytes =
-      2 * xbuf * sizeof(float2) + L::kTwiddleBytes + screen * sizeof(float2) + 32 * sizeof(float);
+      (xbuf + xbuf % 2) * sizeof(float2) + L::kTwiddleBytes + screen * sizeof(float2) + 32 * sizeof(float);
 };
 
 template <class L, int LINES>
-__global__ void __launch_bounds__(LINES * L::R2, 2) persistent_kernel(Params p) {
+__global__ void __launch_bounds__(LINES * L::R2, (L::R1 > 16 ? 256 : 512) / (LINES * L::R2)) persistent_kernel(Params p) {
   extern __shared__ float4 smem_raw[];
   float2* xa = reinterpret_cast<float2*>(smem_raw);
-  float2* xb = xa + Smem<L, LINES>::xbuf;
-  auto* twf = reinterpret_cast<typename L::CF*>(xb + Smem<L, LINES>::xbuf);
+  float2* xb = xa;
+  auto* twf = reinterpret_cast<typename L::CF*>(xa + Smem<L, LINES>::xbuf + Smem<L, LINES>::xbuf % 2);
   auto* twi = reinterpret_cast<typename L::CI*>(reinterpret_cast<char*>(twf) + (L::kFft ? L::N * sizeof(typename L::CF) : 0));
   float2* scr_s = reinterpret_cast<float2*>(reinterpret_cast<char*>(twi) + (L::kFft ? L::N * sizeof(typename L::CI) : 0));
   float* red = reinterpret_cast<float*>(scr_s + Smem<L, LINES>::screen);
   __shared__ long long s_item;
   __shared__ int s_abort;
   fill_twiddles<L>(twf, twi);
+  if (threadIdx.x == 0) s_item = (long long)atomicAdd(p.head, 1u);
   __syncthreads();
   while (true) {
-    if (threadIdx.x == 0) s_item = (long long)atomicAdd(p.head, 1u);
-    __syncthreads();
     const long long item = s_item;
     if (item >= p.total_items) break;
+    // Claim the next item now; the value is only consumed at the end of this
+    // one, so the atomic's round trip overlaps the work below.
+    unsigned next = 0;
+    if (threadIdx.x == 0) next = atomicAdd(p.head, 1u);
     Item it;
     const bool live = decode(p, item, it);
     if (live) {
@@ -335,20 +341,24 @@ __global__ void __launch_bounds__(LINES * L::R2, 2) persistent_kernel(Params p) 
       process<L, LINES>(p, it, xa, xb, twf, twi, red, scr_s);
       __syncthreads();
       if (threadIdx.x == 0) {
-        __threadfence();
+        // release: the CTA's field stores (ordered by the barrier) become
+        // visible before the counter that publishes them
+        asm volatile("fence.acq_rel.gpu;" ::: "memory");
         atomicAdd(p.counters + it.slot, 1u);
       }
     }
-    __syncthreads();  // s_item is rewritten next iteration
+    __syncthreads();  // every thread has read s_item
+    if (threadIdx.x == 0) s_item = (long long)next;
+    __syncthreads();
   }
 }
 
 template <class L, int LINES>
-__global__ void __launch_bounds__(LINES * L::R2, 2) batched_kernel(Params p) {
+__global__ void __launch_bounds__(LINES * L::R2, (L::R1 > 16 ? 256 : 512) / (LINES * L::R2)) batched_kernel(Params p) {
   extern __shared__ float4 smem_raw[];
   float2* xa = reinterpret_cast<float2*>(smem_raw);
-  float2* xb = xa + Smem<L, LINES>::xbuf;
-  auto* twf = reinterpret_cast<typename L::CF*>(xb + Smem<L, LINES>::xbuf);
+  float2* xb = xa;
+  auto* twf = reinterpret_cast<typename L::CF*>(xa + Smem<L, LINES>::xbuf + Smem<L, LINES>::xbuf % 2);
   auto* twi = reinterpret_cast<typename L::CI*>(reinterpret_cast<char*>(twf) + (L::kFft ? L::N * sizeof(typename L::CF) : 0));
   float2* scr_s = reinterpret_cast<float2*>(reinterpret_cast<char*>(twi) + (L::kFft ? L::N * sizeof(typename L::CI) : 0));
   float* red = reinterpret_cast<float*>(scr_s + Smem<L, LINES>::screen);
@@ -374,16 +384,16 @@ struct Config {
 
 bool fft_size(int n) { return n == 64 || n == 128 || n == 256 || n == 512; }
 
-// Lines per CTA for a window; dense windows use 16 lines of 16 threads.
+// Lines per CTA for a window; dense windows use 8 lines of 16 threads.
 bool line_config(int n, Config& c) {
   switch (n) {
-    case 64: c = {8, 8, 32}; return true;
-    case 128: c = {16, 8, 32}; return true;
-    case 256: c = {16, 16, 16}; return true;
-    case 512: c = {32, 16, 8}; return true;
+    case 64: c = {8, 8, kLines64}; return true;
+    case 128: c = {16, 8, kLines128}; return true;
+    case 256: c = {16, 16, kLines256}; return true;
+    case 512: c = {32, 16, kLines512}; return true;
     default:
       if (n >= 2 && n <= 512 && n % 2 == 0) {
-        c = {n <= 128 ? 8 : 32, 16, 16};
+        c = {n <= 128 ? 8 : 32, 16, kLinesDense};
         return true;
       }
       return false;
@@ -436,10 +446,10 @@ int launch_batched(Params& p, int stage, int k, int site0, int batch, cudaStream
 template <class CF, class CI>
 int launch_batched_fft(Params& p, int stage, int k, int site0, int batch, cudaStream_t s) {
   switch (p.st[stage].size) {
-    case 64: return launch_batched<FftLine<8, 8, CF, CI>, 32>(p, stage, k, site0, batch, s);
-    case 128: return launch_batched<FftLine<16, 8, CF, CI>, 32>(p, stage, k, site0, batch, s);
-    case 256: return launch_batched<FftLine<16, 16, CF, CI>, 16>(p, stage, k, site0, batch, s);
-    default: return launch_batched<FftLine<32, 16, CF, CI>, 8>(p, stage, k, site0, batch, s);
+    case 64: return launch_batched<FftLine<8, 8, CF, CI>, kLines64>(p, stage, k, site0, batch, s);
+    case 128: return launch_batched<FftLine<16, 8, CF, CI>, kLines128>(p, stage, k, site0, batch, s);
+    case 256: return launch_batched<FftLine<16, 16, CF, CI>, kLines256>(p, stage, k, site0, batch, s);
+    default: return launch_batched<FftLine<32, 16, CF, CI>, kLines512>(p, stage, k, site0, batch, s);
   }
 }
 
@@ -454,8 +464,8 @@ int launch_batched_any(Params& p, int stage, int k, int site0, int batch, cudaSt
       if (p.precision == MM_PRECISION_MIXED) return launch_batched_fft<float2, double2>(p, stage, k, site0, batch, s);
       return launch_batched_fft<float2, float2>(p, stage, k, site0, batch, s);
     default:
-      if (n <= 128) return launch_batched<DenseLine<8>, 16>(p, stage, k, site0, batch, s);
-      return launch_batched<DenseLine<32>, 16>(p, stage, k, site0, batch, s);
+      if (n <= 128) return launch_batched<DenseLine<8>, kLinesDense>(p, stage, k, site0, batch, s);
+      return launch_batched<DenseLine<32>, kLinesDense>(p, stage, k, site0, batch, s);
   }
 }
 
@@ -482,17 +492,17 @@ int launch_persistent(Params& p, cudaStream_t s) {
 template <class CF, class CI>
 int launch_persistent_fft(Params& p, cudaStream_t s) {
   switch (p.n) {
-    case 64: return launch_persistent<FftLine<8, 8, CF, CI>, 32>(p, s);
-    case 128: return launch_persistent<FftLine<16, 8, CF, CI>, 32>(p, s);
-    case 256: return launch_persistent<FftLine<16, 16, CF, CI>, 16>(p, s);
-    default: return launch_persistent<FftLine<32, 16, CF, CI>, 8>(p, s);
+    case 64: return launch_persistent<FftLine<8, 8, CF, CI>, kLines64>(p, s);
+    case 128: return launch_persistent<FftLine<16, 8, CF, CI>, kLines128>(p, s);
+    case 256: return launch_persistent<FftLine<16, 16, CF, CI>, kLines256>(p, s);
+    default: return launch_persistent<FftLine<32, 16, CF, CI>, kLines512>(p, s);
   }
 }
 
 int launch_persistent_any(Params& p, cudaStream_t s) {
   if (!fft_size(p.n) || p.n != p.n2) {
-    if (std::max(p.n, p.n2) <= 128) return launch_persistent<DenseLine<8>, 16>(p, s);
-    return launch_persistent<DenseLine<32>, 16>(p, s);
+    if (std::max(p.n, p.n2) <= 128) return launch_persistent<DenseLine<8>, kLinesDense>(p, s);
+    return launch_persistent<DenseLine<32>, kLinesDense>(p, s);
   }
   if (p.precision == MM_PRECISION_FP64) return launch_persistent_fft<double2, double2>(p, s);
   if (p.precision == MM_PRECISION_MIXED) return launch_persistent_fft<float2, double2>(p, s);
