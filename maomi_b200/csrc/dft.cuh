@@ -197,10 +197,13 @@ struct FftLine {
   static constexpr int N = R1 * R2;
   static constexpr int J = R1 / R2;  // columns of the second pass per thread
   static constexpr int PITCH = R2 + 1;
-  // float2 per line per buffer: padded to 1 (mod 16) so consecutive lines
-  // start on consecutive 8-byte bank pairs; in the column layout a warp holds
-  // 16-32 different lines at the same in-line offset.
-  static constexpr int XBUF = (R1 * PITCH + 15) / 16 * 16 + 1;
+  // float2 per line per buffer.  In the column layout a warp holds 8-16
+  // lines at the same in-line offset, in the row layout 2-4 lines at
+  // consecutive offsets; the line stride (mod 16 eight-byte bank pairs) is
+  // chosen so both layouts reach the fewest shared-memory wavefronts for the
+  // CTA shapes of the propagation kernel (8 lines for R2 = 16, 16 for R2 = 8).
+  static constexpr int kStrideResidue = R2 == 16 ? 2 : (R1 == 16 ? 3 : 10);
+  static constexpr int XBUF = R1 * PITCH + ((kStrideResidue - (R1 * PITCH) % 16) + 16) % 16;
   static constexpr bool kFft = true;
   static constexpr size_t kTwiddleBytes = (size_t)N * (sizeof(CF) + sizeof(CI));
   static_assert(R1 % R2 == 0, "R2 must divide R1");
@@ -208,9 +211,15 @@ struct FftLine {
   // twf[k1*R2 + t] = W_N^(t*k1) (CF);  twi[n*R1 + k1] = W_N^(-n*k1) (CI).
   // SINGLE: xa and xb are the same buffer; two more barriers keep the
   // exchanges apart (and the next call's first exchange after this one's last).
+  // warp_local: the line's R2 threads share one warp (row layout), so a warp
+  // barrier orders the exchanges; otherwise the whole CTA synchronises.
   template <bool SINGLE = false>
   __device__ static void propagate(float2 (&x)[R1], int t, const float2* __restrict__ q, int /*n*/,
-                                   float2* xa, float2* xb, const CF* twf, const CI* twi) {
+                                   float2* xa, float2* xb, const CF* twf, const CI* twi, bool warp_local = false) {
+    auto sync = [warp_local]() {
+      if (warp_local) __syncwarp();
+      else __syncthreads();
+    };
     CF v[R1];
 #pragma unroll
     for (int m = 0; m < R1; ++m) v[m] = from_f2<CF>(x[m]);
@@ -220,7 +229,7 @@ struct FftLine {
     for (int k1 = 1; k1 < R1; ++k1) v[k1] = cmul(v[k1], twf[k1 * R2 + t]);
 #pragma unroll
     for (int k1 = 0; k1 < R1; ++k1) xa[k1 * PITCH + t] = to_f2(v[k1]);
-    __syncthreads();
+    sync();
     // ---- forward pass 2: thread t owns k1 = t + R2*j
 #pragma unroll
     for (int j = 0; j < J; ++j)
@@ -238,7 +247,7 @@ struct FftLine {
     // ---- inverse pass 1: IDFT over k2 -> n_a, twiddle W_N^(-n_a*k1), exchange
 #pragma unroll
     for (int j = 0; j < J; ++j) dft<R2, +1>(w + j * R2);
-    if constexpr (SINGLE) __syncthreads();  // forward reads of the shared buffer done
+    if constexpr (SINGLE) sync();  // forward reads of the shared buffer done
 #pragma unroll
     for (int j = 0; j < J; ++j)
 #pragma unroll
@@ -248,14 +257,14 @@ struct FftLine {
         if (na) z = cmul(z, twi[na * R1 + k1]);
         xb[k1 * PITCH + na] = to_f2(z);
       }
-    __syncthreads();
+    sync();
     // ---- inverse pass 2: thread t = n_a gathers every k1
 #pragma unroll
     for (int k1 = 0; k1 < R1; ++k1) w[k1] = from_f2<CI>(xb[k1 * PITCH + t]);
     dft<R1, +1>(w);
 #pragma unroll
     for (int m = 0; m < R1; ++m) x[m] = to_f2(w[m]);
-    if constexpr (SINGLE) __syncthreads();  // inverse reads done before the buffer is reused
+    if constexpr (SINGLE) sync();  // inverse reads done before the buffer is reused
   }
 };
 
@@ -277,7 +286,7 @@ struct DenseLine {
 
   template <bool SINGLE = false>
   __device__ static void propagate(float2 (&v)[R1], int t, const float2* __restrict__ ker, int n, float2* xa,
-                                   float2* /*xb*/, const CF* /*twf*/, const CI* /*twi*/) {
+                                   float2* /*xb*/, const CF* /*twf*/, const CI* /*twi*/, bool /*warp_local*/ = false) {
 #pragma unroll
     for (int j = 0; j < R1; ++j) {
       const int e = t + R2 * j;

@@ -162,14 +162,15 @@ __device__ void prefetch_screen(const Params& p, const Item& it, float2* scr_s) 
   const Lane<L, LINES> ln(p, it);
   const int N = st.size;
   const int2 o = site_offset(p, it);
-  const float2* scr = st.screens + (size_t)it.k * st.vol_h * st.vol_w;
+  // element j of this thread sits at base + j*step in the (vol_h, vol_w) plane
+  const int row0 = ln.axis == 0 ? ln.line : ln.t, col0 = ln.axis == 0 ? ln.t : ln.line;
+  const float2* scr = st.screens + (size_t)it.k * st.vol_h * st.vol_w + (size_t)(o.x + row0) * st.vol_w + (o.y + col0);
+  const size_t step = ln.axis == 0 ? size_t(L::R2) : size_t(L::R2) * st.vol_w;
 #pragma unroll
   for (int j = 0; j < L::R1; ++j) {
     const int e = ln.t + L::R2 * j;
     if (!(L::kFft || (ln.line < N && e < N))) continue;
-    const int row = ln.axis == 0 ? ln.line : e;
-    const int col = ln.axis == 0 ? e : ln.line;
-    cp_async8(scr_s + j * blockDim.x + threadIdx.x, scr + (size_t)(o.x + row) * st.vol_w + (o.y + col));
+    cp_async8(scr_s + j * blockDim.x + threadIdx.x, scr + j * step);
   }
   cp_async_commit();
 }
@@ -190,36 +191,48 @@ __device__ void process(const Params& p, const Item& it, float2* xa, float2* xb,
   const bool live = L::kFft || line < N;
   auto in_line = [&](int e) { return L::kFft || (live && e < N); };
 
+  // Element j of this thread: (row, col) = (row0, col0) + j * (drow, dcol).
+  const int row0 = axis == 0 ? line : t, col0 = axis == 0 ? t : line;
+  const int drow = axis == 0 ? 0 : R2, dcol = axis == 0 ? R2 : 0;
+  const int jstep = axis == 0 ? R2 : R2 * N;  // linear step in an N x N buffer
+
   float2 v[R1];
   // ------------------------------------------------------------------ load
   {
     const size_t slot_a = (size_t)it.slot * p.n * p.n;
     const size_t slot_b = (size_t)it.slot * p.n2 * p.n2;
+    if (it.k > 0 || it.stage == 0) {
+      const float2* src = it.k == 0 ? p.base : (it.stage == 1 ? p.bufB + slot_b : p.bufA + slot_a);
+      src += (size_t)row0 * N + col0;
 #pragma unroll
-    for (int j = 0; j < R1; ++j) {
-      const int e = t + R2 * j;
-      const int row = axis == 0 ? line : e;
-      const int col = axis == 0 ? e : line;
-      float2 a = make_float2(0.f, 0.f);
-      if (!in_line(e)) {
-      } else if (it.k > 0) {
-        const float2* buf = (it.stage == 1) ? p.bufB + slot_b : p.bufA + slot_a;
-        a = __ldcg(buf + (size_t)row * N + col);
-      } else if (it.stage == 0) {
-        a = __ldg(p.base + (size_t)row * N + col);
-      } else if (it.stage == 1) {
-        a = __ldcg(p.bufA + slot_a + (size_t)(row + p.crop0) * p.n + (col + p.crop0));
-      } else {
-        const int r2 = row - p.crop0, c2 = col - p.crop0;
-        a = (r2 >= 0 && r2 < p.n2 && c2 >= 0 && c2 < p.n2)
-                ? __ldcg(p.bufB + slot_b + (size_t)r2 * p.n2 + c2)
-                : make_float2(0.f, 0.f);
+      for (int j = 0; j < R1; ++j) {
+        v[j] = make_float2(0.f, 0.f);
+        if (!in_line(t + R2 * j)) continue;
+        v[j] = it.k == 0 ? __ldg(src + (size_t)j * jstep) : __ldcg(src + (size_t)j * jstep);
       }
-      v[j] = a;
+    } else if (it.stage == 1) {  // crop the n x n field of stage A to the n2 window
+      const float2* src = p.bufA + slot_a + (size_t)(row0 + p.crop0) * p.n + (col0 + p.crop0);
+      const int step_n = axis == 0 ? R2 : R2 * p.n;
+#pragma unroll
+      for (int j = 0; j < R1; ++j) {
+        v[j] = make_float2(0.f, 0.f);
+        if (in_line(t + R2 * j)) v[j] = __ldcg(src + (size_t)j * step_n);
+      }
+    } else {  // zero-pad the n2 field of stage B to the n window
+#pragma unroll
+      for (int j = 0; j < R1; ++j) {
+        const int r2 = row0 + j * drow - p.crop0, c2 = col0 + j * dcol - p.crop0;
+        v[j] = (in_line(t + R2 * j) && r2 >= 0 && r2 < p.n2 && c2 >= 0 && c2 < p.n2)
+                   ? __ldcg(p.bufB + slot_b + (size_t)r2 * p.n2 + c2)
+                   : make_float2(0.f, 0.f);
+      }
     }
   }
   // ---------------------------------------- second half of step k-1
-  if (it.k > 0) L::template propagate<true>(v, t, st.kern + (size_t)(it.k - 1) * N, N, xa_l, xb_l, twf, twi);
+  // Row layout keeps each line inside one warp: its exchanges need only warp barriers.
+  const bool warp_local = L::kFft && axis == 0 && 32 % R2 == 0;
+  if (it.k > 0)
+    L::template propagate<true>(v, t, st.kern + (size_t)(it.k - 1) * N, N, xa_l, xb_l, twf, twi, warp_local);
   // ------------------------------------------------------- screen of step k
   if (it.k < st.steps) {
     const float eline = live ? __ldg(st.edge + line) : 0.f;
@@ -244,15 +257,16 @@ __device__ void process(const Params& p, const Item& it, float2* xa, float2* xb,
       float* img = p.tail_img[tail] + (size_t)(p.tail_per_site ? it.site : it.slot) * p.n2 * p.n2;
       const bool init = p.tail_per_site && pt == 0;
       float psum = 0.f;
+      // the line must cross the centred n2 crop; then test the in-line coordinate
+      const int lc = line - p.crop0;
+      if (live && lc >= 0 && lc < p.n2) {
 #pragma unroll
-      for (int j = 0; j < R1; ++j) {
-        const int e = t + R2 * j;
-        const int r2 = (axis == 0 ? line : e) - p.crop0;
-        const int c2 = (axis == 0 ? e : line) - p.crop0;
-        if (in_line(e) && r2 >= 0 && r2 < p.n2 && c2 >= 0 && c2 < p.n2) {
+        for (int j = 0; j < R1; ++j) {
+          const int ec = t + R2 * j - p.crop0;
+          if (!in_line(t + R2 * j) || ec < 0 || ec >= p.n2) continue;
           const float pw = photon_power(v[j], p.order);
           psum += pw;
-          float* dst = img + (size_t)r2 * p.n2 + c2;
+          float* dst = img + (axis == 0 ? (size_t)lc * p.n2 + ec : (size_t)ec * p.n2 + lc);
           const float prev = init ? 0.f : __ldcg(dst);
           __stcg(dst, prev + wgt * pw);
         }
@@ -261,28 +275,29 @@ __device__ void process(const Params& p, const Item& it, float2* xa, float2* xb,
       if (threadIdx.x == 0) atomicAdd(p.profile[tail] + (size_t)it.site * p.planes[tail] + pt, (double)tot);
     } else if (it.stage == 1 && it.k < st.steps) {
       float* dst = p.focal + ((size_t)it.site * st.steps + it.k) * p.fh * p.fw;
+      const int lf = line - (axis == 0 ? p.fx0 : p.fy0);            // line inside the focal crop?
+      const int lext = axis == 0 ? p.fh : p.fw, eorg = axis == 0 ? p.fy0 : p.fx0, eext = axis == 0 ? p.fw : p.fh;
+      if (live && lf >= 0 && lf < lext) {
 #pragma unroll
-      for (int j = 0; j < R1; ++j) {
-        const int e = t + R2 * j;
-        const int r = (axis == 0 ? line : e) - p.fx0;
-        const int c = (axis == 0 ? e : line) - p.fy0;
-        if (in_line(e) && r >= 0 && r < p.fh && c >= 0 && c < p.fw) __stcs(dst + (size_t)r * p.fw + c, photon_power(v[j], p.order));
+        for (int j = 0; j < R1; ++j) {
+          const int ef = t + R2 * j - eorg;
+          if (!in_line(t + R2 * j) || ef < 0 || ef >= eext) continue;
+          const size_t off = axis == 0 ? (size_t)lf * p.fw + ef : (size_t)ef * p.fw + lf;
+          __stcs(dst + off, photon_power(v[j], p.order));
+        }
       }
     }
   }
   // ---------------------------------------- first half of step k
-  if (it.k < st.steps) L::template propagate<true>(v, t, st.kern + (size_t)it.k * N, N, xa_l, xb_l, twf, twi);
+  if (it.k < st.steps)
+    L::template propagate<true>(v, t, st.kern + (size_t)it.k * N, N, xa_l, xb_l, twf, twi, warp_local);
   // ------------------------------------------------------------------ store
   if (!(it.stage == 2 && it.k == st.steps)) {
-    float2* buf = (it.stage == 1) ? p.bufB + (size_t)it.slot * p.n2 * p.n2 : p.bufA + (size_t)it.slot * p.n * p.n;
+    float2* dst = (it.stage == 1 ? p.bufB + (size_t)it.slot * p.n2 * p.n2 : p.bufA + (size_t)it.slot * p.n * p.n) +
+                  (size_t)row0 * N + col0;
 #pragma unroll
-    for (int j = 0; j < R1; ++j) {
-      const int e = t + R2 * j;
-      if (!in_line(e)) continue;
-      const int row = axis == 0 ? line : e;
-      const int col = axis == 0 ? e : line;
-      __stcg(buf + (size_t)row * N + col, v[j]);
-    }
+    for (int j = 0; j < R1; ++j)
+      if (in_line(t + R2 * j)) __stcg(dst + (size_t)j * jstep, v[j]);
   }
 }
 
