@@ -211,6 +211,42 @@ int mm_propagate_sites(const mm_stage_plan* plan, int schedule, int slots, void*
 int mm_propagate_sites_noalloc(const mm_stage_plan* plan, int schedule, int slots, int check, void* stream);
 
 /* ------------------------------------------------------------------------
+ * Independent propagation items of one window size (uneven depths) in one
+ * persistent launch: item i propagates field_in through steps[i] screens
+ * exp(1j*phase) (times an optional separable edge window), one step being
+ * u <- IDFT2(Q * DFT2(u * screen)) with a 1-D transfer function `kernel`
+ * applied along both axes.  Generalises the split-step loop of
+ * maomi/numerics.py:189-206 (constant pitch) to a device work queue of
+ * many items; the reference propagates such items one call at a time.
+ * Items are processed in waves of `slots` (sort them by depth); the schedule
+ * tables come from the caller (see maomi_b200/items.py).
+ */
+typedef struct {
+  int n;                       /* window: 64, 128, 256 or 512                     */
+  int nitems;
+  int slots;                   /* items in flight (one wave)                      */
+  int waves;
+  long long total_items;       /* queue length = wave_items[waves]                */
+  const int32_t* steps;        /* device (nitems)                                 */
+  const int64_t* phase_offset; /* device (nitems): float offset of each (steps,n,n) stack */
+  const float* phase;          /* device: flat phase stacks (radians)             */
+  const void* field_in;        /* device float2 (n,n)                             */
+  void* field_out;             /* device float2 (nitems,n,n)                      */
+  const void* kernel;          /* device float2 (n): FFT order, 1/n folded in      */
+  const float* edge1d;         /* device (n) or NULL                              */
+  const int64_t* wave_items;   /* device (waves+1): first queue item of each wave */
+  const int32_t* wave_levels;  /* device (waves): segments per wave (max steps+1) */
+  const int32_t* slot_base;    /* device (waves*slots): counter before each wave  */
+  int precision;               /* MM_PRECISION_*                                  */
+  int shape;                   /* CTA shape: 0 default radices, 1 wider per thread */
+} mm_item_class;
+
+/* Line blocks per segment for window n and CTA shape (for the schedule). */
+int mm_items_blocks(int n, int shape);
+size_t mm_propagate_items_workspace_size(const mm_item_class* c);
+int mm_propagate_items(const mm_item_class* c, void* workspace, size_t workspace_bytes, int check, void* stream);
+
+/* ------------------------------------------------------------------------
  * Focal PSF finalisation: psf[p,x,y,z] = scale*axial[z] *
  *   sum_i wx[x,i] sum_j wy[y,j] focal[p,z,ix[x,i],iy[y,j]]
  * from the focal |E|^(2*order) crops (sparse resample tables as ResamplePlan

@@ -35,6 +35,13 @@ class StagePlan(Structure):
                 ("precision", c_int)]
 
 
+class ItemClass(Structure):
+    _fields_ = [("n", c_int), ("nitems", c_int), ("slots", c_int), ("waves", c_int), ("total_items", ctypes.c_longlong),
+                ("steps", c_void_p), ("phase_offset", c_void_p), ("phase", c_void_p), ("field_in", c_void_p),
+                ("field_out", c_void_p), ("kernel", c_void_p), ("edge1d", c_void_p), ("wave_items", c_void_p),
+                ("wave_levels", c_void_p), ("slot_base", c_void_p), ("precision", c_int), ("shape", c_int)]
+
+
 class PupilDesc(Structure):
     _fields_ = [("n", c_int), ("pitch", c_double), ("beam_radius", c_double), ("aperture", c_double),
                 ("k", c_double), ("focal_length", c_double), ("nmodes", c_int), ("mode_coef", c_double_p),
@@ -73,6 +80,9 @@ SIGNATURES = {
     "mm_propagate_workspace_size": (c_size_t, [POINTER(StagePlan), c_int, c_int]),
     "mm_propagate_sites": (c_int, [POINTER(StagePlan), c_int, c_int, c_void_p, c_size_t, c_int, c_void_p]),
     "mm_propagate_sites_noalloc": (c_int, [POINTER(StagePlan), c_int, c_int, c_int, c_void_p]),
+    "mm_items_blocks": (c_int, [c_int, c_int]),
+    "mm_propagate_items_workspace_size": (c_size_t, [POINTER(ItemClass)]),
+    "mm_propagate_items": (c_int, [POINTER(ItemClass), c_void_p, c_size_t, c_int, c_void_p]),
     "mm_focal_finalize": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_int, c_void_p, c_float,
                                   c_int, c_int, c_int, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p,
                                   c_void_p]),

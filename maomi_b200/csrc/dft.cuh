@@ -201,8 +201,9 @@ struct FftLine {
   // lines at the same in-line offset, in the row layout 2-4 lines at
   // consecutive offsets; the line stride (mod 16 eight-byte bank pairs) is
   // chosen so both layouts reach the fewest shared-memory wavefronts for the
-  // CTA shapes of the propagation kernel (8 lines for R2 = 16, 16 for R2 = 8).
-  static constexpr int kStrideResidue = R2 == 16 ? 2 : (R1 == 16 ? 3 : 10);
+  // CTA shapes of the propagation kernels (128 threads: 8 lines for R2 = 16,
+  // 16 for R2 = 8, 32 for R2 = 4).
+  static constexpr int kStrideResidue = R2 == 16 ? 2 : (R1 == 8 ? (R2 == 8 ? 10 : 9) : 3);
   static constexpr int XBUF = R1 * PITCH + ((kStrideResidue - (R1 * PITCH) % 16) + 16) % 16;
   static constexpr bool kFft = true;
   static constexpr size_t kTwiddleBytes = (size_t)N * (sizeof(CF) + sizeof(CI));
