@@ -238,7 +238,8 @@ def main():
     kernel_ms = float(np.mean([a.elapsed_time(b) for a, b in kev]))
     if args.no_e2e:
         if rank == 0:
-            print(json.dumps({"profile_case": True, "sites": len(points), "ms_per_step": ms, "kernel_ms": kernel_ms}))
+            print(json.dumps({"profile_case": True, "sites": len(points), "ms_per_step": ms, "kernel_ms": kernel_ms,
+                              "schedule": args.schedule, "slots": args.slots}))
         return
     # ---- end to end through the public API with host buffers
     probe = step(raw_dev)
