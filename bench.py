@@ -37,6 +37,11 @@ FOCAL_BYTES = 4 * 40 * 40 * 46
 # algorithmic bytes per site: per step one complex64 field read + write and one
 # complex64 screen read (24 n^2), plus the float32 focal PSF written once
 BYTES_PER_SITE = SCREEN_STEPS * 24 * WINDOW * WINDOW + FOCAL_BYTES
+# DRAM bytes (read + write) per site of the propagation kernel, from an ncu
+# capture of a 64-site case (dram__bytes_read.sum + dram__bytes_write.sum =
+# 245.8 MB); traffic grows with the sites processed, so a launch moves this
+# figure times its sites.  The fields of the sites in flight stay in L2.
+NCU_DRAM_BYTES_PER_SITE = 245.8e6 / 64
 METRIC = "propagated sites/s at 512^2x60 (plain optical stage incl. tails + v4 mask)"
 
 
@@ -52,7 +57,7 @@ def parse():
     ap.add_argument("--cpu-sites", type=int, default=8)
     ap.add_argument("--sites", type=int, default=SITES, help="profile a subset of the lattice (not a bench line)")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64", "fp32"])
+    ap.add_argument("--precision", default="compensated", choices=["compensated", "mixed", "fp64", "fp32"])
     return ap.parse_args()
 
 
@@ -282,7 +287,9 @@ def main():
                     "d2h_bytes_per_step": int(d2h)},
             "gpu_launches": int(round(launches)),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
-                         "frac": achieved / pk["hbm_gbs"], "traffic": None,
+                         "frac": achieved / pk["hbm_gbs"],
+                         "traffic": len(points) * NCU_DRAM_BYTES_PER_SITE,
+                         "traffic_source": "ncu capture of 64 sites, scaled by sites",
                          "kernel": "mm propagation (persistent)", "kernel_ms": kernel_ms,
                          "bytes_per_launch": len(points) * BYTES_PER_SITE, "peak_source": pk_kind},
             "clocks": clk.summary(),

@@ -176,12 +176,14 @@ typedef struct {
   const int32_t* offsets;  /* (P,2) window offsets on the screen lattice          */
   int nsites;
   int precision;           /* arithmetic of the radix-2 line transforms: FP32,
-                              FP64 (butterflies, twiddles and filter in FP64) or
-                              MIXED (forward FP32, inverse FP64); the field is
-                              stored complex64 in every mode                      */
+                              FP64 (butterflies, twiddles and filter in FP64),
+                              MIXED (forward FP32, inverse FP64) or COMPENSATED
+                              (FP32 butterflies, every DFT rotation and twiddle
+                              constant carried as a hi + lo pair of floats); the
+                              field is stored complex64 in every mode             */
 } mm_stage_plan;
 
-enum { MM_PRECISION_FP32 = 0, MM_PRECISION_FP64 = 1, MM_PRECISION_MIXED = 2 };
+enum { MM_PRECISION_FP32 = 0, MM_PRECISION_FP64 = 1, MM_PRECISION_MIXED = 2, MM_PRECISION_COMPENSATED = 3 };
 
 enum { MM_SCHEDULE_PERSISTENT = 0, MM_SCHEDULE_BATCHED = 1 };
 
@@ -298,6 +300,18 @@ size_t mm_local_render_workspace_size(const mm_local_desc* desc);
 int mm_local_render(const mm_local_desc* desc, const double* source /* (sx,sy,sz) */,
                     const double* zweight /* (sz) or NULL */, double* out /* (sx,sy[,sz]) */,
                     void* workspace, size_t workspace_bytes, void* stream);
+
+/* ------------------------------------------------------------------------
+ * BF16 tensor-core GEMM (tcgen05, FP32 accumulation), the building block of
+ * the surrogate's spectral and pointwise layers:
+ *   d[m x n] (FP32, row-major) = a[m x k] * b[n x k]^T   (a, b BF16, row-major)
+ * n and k multiples of 16; a and b 16-byte aligned.  `err` is a zeroed device
+ * int that a timed-out pipeline wait sets.  No reference counterpart: the
+ * reference's surrogate-free stage has no GEMM; this is the kernel the
+ * planned mm_surrogate_* entry points are built on, exported for testing.
+ */
+int mm_gemm_bf16_tn(const void* a, const void* b, float* d, int m, int n, int k, int* err, int check,
+                    void* stream);
 
 #ifdef __cplusplus
 }

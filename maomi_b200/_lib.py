@@ -14,8 +14,9 @@ LIB_PATH = Path(__file__).resolve().parent / "libmaomi_b200.so"
 
 MM_OK, MM_ERR_ARGUMENT, MM_ERR_CUDA, MM_ERR_TIMEOUT, MM_ERR_NONFINITE, MM_ERR_UNSUPPORTED = 0, -1, -2, -3, -4, -5
 MM_SCHEDULE_PERSISTENT, MM_SCHEDULE_BATCHED = 0, 1
-MM_PRECISION_FP32, MM_PRECISION_FP64, MM_PRECISION_MIXED = 0, 1, 2
-PRECISIONS = {"fp32": MM_PRECISION_FP32, "fp64": MM_PRECISION_FP64, "mixed": MM_PRECISION_MIXED}
+MM_PRECISION_FP32, MM_PRECISION_FP64, MM_PRECISION_MIXED, MM_PRECISION_COMPENSATED = 0, 1, 2, 3
+PRECISIONS = {"fp32": MM_PRECISION_FP32, "fp64": MM_PRECISION_FP64, "mixed": MM_PRECISION_MIXED,
+              "compensated": MM_PRECISION_COMPENSATED}
 
 c_int_p = POINTER(c_int)
 c_float_p = POINTER(c_float)
@@ -67,6 +68,7 @@ SIGNATURES = {
     "mm_last_error": (c_char_p, []),
     "mm_device_supported": (c_int, []),
     "mm_launch_count": (ctypes.c_ulonglong, []),
+    "mm_gemm_bf16_tn": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, c_int, c_void_p, c_int, c_void_p]),
     "mm_gather_screens": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int, c_int, c_int, c_int, c_void_p]),
     "mm_resample_power": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int,
                                   c_int, c_int, c_int, c_int, c_int, c_int, c_int, c_float, c_void_p]),

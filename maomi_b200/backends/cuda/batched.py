@@ -69,11 +69,11 @@ class ResampleTables:
 class OpticalPlan:
     """Persistent device state of the optical stage for one configuration."""
 
-    def __init__(self, config, raw_fields, *, uin=None, device="cuda", native=True, precision="fp64"):
+    def __init__(self, config, raw_fields, *, uin=None, device="cuda", native=True, precision="compensated"):
         import torch
         _lib.require_cuda(device)
         if precision not in _lib.PRECISIONS:
-            raise ValueError("precision must be fp32, mixed or fp64")
+            raise ValueError("precision must be one of " + ", ".join(_lib.PRECISIONS))
         #: arithmetic of the radix-2 line transforms: "fp64" (FP64 butterflies,
         #: twiddles and filter), "mixed" (forward FP32, inverse FP64) or "fp32";
         #: fields are stored complex64 in every mode

@@ -15,6 +15,8 @@
 // forward transform produces, and the inverse consumes that order.
 #pragma once
 
+#include <type_traits>
+
 #include "common.cuh"
 
 namespace mm {
@@ -37,6 +39,7 @@ __device__ constexpr double kSin16[17] = {
 template <class C> struct Real;
 template <> struct Real<float2> { using T = float; };
 template <> struct Real<double2> { using T = double; };
+template <> struct Real<cfx> { using T = float; };
 
 // a * W_32^k with W = exp(SIGN * 2*pi*i/32), k = 0..15 (angle pi*k/16).
 template <int SIGN, int K, class C>
@@ -46,6 +49,21 @@ __device__ __forceinline__ C rot32(C a) {
     return a;
   } else if constexpr (K == 8) {
     return quarter<SIGN>(a);
+  } else if constexpr (std::is_same_v<C, cfx>) {
+    // constants as hi + lo float pairs (see cfx)
+    constexpr double c = kCos16[K], s = SIGN * kSin16[K];
+    constexpr float ch = float(c), sh = float(s);
+    constexpr float cl = float(c - double(ch)), sl = float(s - double(sh));
+    if constexpr (K == 4 || K == 12) {
+      // |c| = |s| = sqrt(1/2): one rounded sum, then the scaled product
+      constexpr float g = c > 0 ? ch : -ch, gl = c > 0 ? cl : -cl;  // +sqrt(1/2) as hi + lo
+      constexpr float ex = c > 0 ? 1.f : -1.f, ey = s > 0 ? 1.f : -1.f;
+      const float u = ex * a.x - ey * a.y, w = ey * a.x + ex * a.y;
+      return cfx{fmaf(u, g, u * gl), fmaf(w, g, w * gl)};
+    } else {
+      const float rx = fmaf(a.x, cl, -a.y * sl), ry = fmaf(a.x, sl, a.y * cl);
+      return cfx{fmaf(a.x, ch, fmaf(-a.y, sh, rx)), fmaf(a.x, sh, fmaf(a.y, ch, ry))};
+    }
   } else {
     const T c = T(kCos16[K]), s = T(SIGN * kSin16[K]);
     C r;
@@ -183,7 +201,8 @@ __device__ __forceinline__ void dft(C* v) {
 // exchange suffices.
 //
 // CF / CI are the register arithmetic types of the forward and the inverse
-// half: float2 (FP32) or double2 (FP64 butterflies, twiddles and filter).
+// half: float2 (FP32), cfx (FP32 butterflies, constants as hi + lo pairs) or
+// double2 (FP64 butterflies, twiddles and filter).
 // The line enters and leaves as complex64 and the exchanges are complex64.
 // The inverse half carries most of the rounding that reaches the saved
 // intensities, so <float2, double2> ("mixed") recovers most of the FP64
@@ -192,6 +211,8 @@ template <int R1_, int R2_, class CF_ = float2, class CI_ = CF_>
 struct FftLine {
   using CF = CF_;
   using CI = CI_;
+  using TF = typename TwiddleOf<CF>::T;  // twiddle-table entries of each half
+  using TI = typename TwiddleOf<CI>::T;
   static constexpr int R1 = R1_;
   static constexpr int R2 = R2_;
   static constexpr int N = R1 * R2;
@@ -206,7 +227,11 @@ struct FftLine {
   static constexpr int kStrideResidue = R2 == 16 ? 2 : (R1 == 8 ? (R2 == 8 ? 10 : 9) : 3);
   static constexpr int XBUF = R1 * PITCH + ((kStrideResidue - (R1 * PITCH) % 16) + 16) % 16;
   static constexpr bool kFft = true;
-  static constexpr size_t kTwiddleBytes = (size_t)N * (sizeof(CF) + sizeof(CI));
+  static constexpr size_t kTwiddleBytes = (size_t)N * (sizeof(TF) + sizeof(TI));
+  // CTAs of 128 threads resident per SM the kernels are compiled for: the
+  // FP32 forms fit in 96 registers (5 CTAs); FP64 halves need the 4-CTA budget.
+  static constexpr int kMinBlocks =
+      R1 > 16 ? 2 : ((std::is_same_v<CF, double2> || std::is_same_v<CI, double2>) ? 4 : 5);
   static_assert(R1 % R2 == 0, "R2 must divide R1");
 
   // twf[k1*R2 + t] = W_N^(t*k1) (CF);  twi[n*R1 + k1] = W_N^(-n*k1) (CI).
@@ -216,7 +241,7 @@ struct FftLine {
   // barrier orders the exchanges; otherwise the whole CTA synchronises.
   template <bool SINGLE = false>
   __device__ static void propagate(float2 (&x)[R1], int t, const float2* __restrict__ q, int /*n*/,
-                                   float2* xa, float2* xb, const CF* twf, const CI* twi, bool warp_local = false) {
+                                   float2* xa, float2* xb, const TF* twf, const TI* twi, bool warp_local = false) {
     auto sync = [warp_local]() {
       if (warp_local) __syncwarp();
       else __syncthreads();
@@ -278,16 +303,19 @@ template <int RMAX>
 struct DenseLine {
   using CF = float2;
   using CI = float2;
+  using TF = float2;
+  using TI = float2;
   static constexpr size_t kTwiddleBytes = 0;
   static constexpr int R1 = RMAX;
   static constexpr int R2 = 16;
   static constexpr int N = RMAX * 16;  // capacity
   static constexpr int XBUF = N + 1;  // odd stride: lines start on different banks
   static constexpr bool kFft = false;
+  static constexpr int kMinBlocks = RMAX > 16 ? 2 : 4;
 
   template <bool SINGLE = false>
   __device__ static void propagate(float2 (&v)[R1], int t, const float2* __restrict__ ker, int n, float2* xa,
-                                   float2* /*xb*/, const CF* /*twf*/, const CI* /*twi*/, bool /*warp_local*/ = false) {
+                                   float2* /*xb*/, const TF* /*twf*/, const TI* /*twi*/, bool /*warp_local*/ = false) {
 #pragma unroll
     for (int j = 0; j < R1; ++j) {
       const int e = t + R2 * j;

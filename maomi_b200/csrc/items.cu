@@ -68,25 +68,25 @@ struct ISmem {
 };
 
 template <class L>
-__device__ void ifill_twiddles(typename L::CF* twf, typename L::CI* twi) {
+__device__ void ifill_twiddles(typename L::TF* twf, typename L::TI* twi) {
   for (int i = threadIdx.x; i < L::N; i += blockDim.x) {
     double s, c;
     const int k1 = i / L::R2, t = i % L::R2;
     sincospi(-2.0 * double((t * k1) % L::N) / L::N, &s, &c);
-    twf[i] = make_c<typename L::CF>(c, s);
+    twf[i] = make_tw<typename L::TF>(c, s);
     const int nn = i / L::R1, k2 = i % L::R1;
     sincospi(2.0 * double((nn * k2) % L::N) / L::N, &s, &c);
-    twi[i] = make_c<typename L::CI>(c, s);
+    twi[i] = make_tw<typename L::TI>(c, s);
   }
 }
 
 template <class L, int LINES>
-__global__ void __launch_bounds__(LINES * L::R2, (L::R1 > 16 ? 256 : 512) / (LINES * L::R2)) items_kernel(ItemP p) {
+__global__ void __launch_bounds__(LINES * L::R2, L::kMinBlocks * 128 / (LINES * L::R2)) items_kernel(ItemP p) {
   constexpr int R1 = L::R1, R2 = L::R2, N = L::N;
   extern __shared__ float4 smem_raw[];
   float2* xa = reinterpret_cast<float2*>(smem_raw);
-  auto* twf = reinterpret_cast<typename L::CF*>(xa + ISmem<L, LINES>::xbuf + ISmem<L, LINES>::xbuf % 2);
-  auto* twi = reinterpret_cast<typename L::CI*>(twf + N);
+  auto* twf = reinterpret_cast<typename L::TF*>(xa + ISmem<L, LINES>::xbuf + ISmem<L, LINES>::xbuf % 2);
+  auto* twi = reinterpret_cast<typename L::TI*>(twf + N);
   float* ph_s = reinterpret_cast<float*>(twi + N);
   __shared__ long long s_item;
   __shared__ int s_abort;
@@ -257,7 +257,7 @@ extern "C" int mm_propagate_items(const mm_item_class* c, void* workspace, size_
   MM_CHECK_ARG(c->nitems >= 0 && c->slots >= 1 && c->waves >= 0, "bad item counts");
   MM_CHECK_ARG(c->shape == 0 || c->shape == 1, "unknown shape %d", c->shape);
   MM_CHECK_ARG(c->precision == MM_PRECISION_FP32 || c->precision == MM_PRECISION_FP64 ||
-                   c->precision == MM_PRECISION_MIXED,
+                   c->precision == MM_PRECISION_MIXED || c->precision == MM_PRECISION_COMPENSATED,
                "unknown precision %d", c->precision);
   if (c->nitems == 0) return MM_OK;
   MM_CHECK_ARG(c->steps && c->phase_offset && c->phase && c->field_in && c->field_out && c->kernel &&
@@ -288,6 +288,7 @@ extern "C" int mm_propagate_items(const mm_item_class* c, void* workspace, size_
   int rc;
   if (c->precision == MM_PRECISION_FP64) rc = ilaunch_any<double2, double2>(p, c->shape, s);
   else if (c->precision == MM_PRECISION_MIXED) rc = ilaunch_any<float2, double2>(p, c->shape, s);
+  else if (c->precision == MM_PRECISION_COMPENSATED) rc = ilaunch_any<cfx, cfx>(p, c->shape, s);
   else rc = ilaunch_any<float2, float2>(p, c->shape, s);
   if (rc != MM_OK || !check) return rc;
   MM_CHECK_CUDA(cudaStreamSynchronize(s), "item propagation");

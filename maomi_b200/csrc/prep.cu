@@ -238,8 +238,8 @@ template <class L, int LINES>
 __global__ void __launch_bounds__(LINES * L::R2) line_pass_kernel(float2* __restrict__ f, int n, int axis,
                                                                   const float2* __restrict__ q) {
   extern __shared__ float4 smem_raw[];
-  using CF = typename L::CF;
-  using CI = typename L::CI;
+  using CF = typename L::TF;
+  using CI = typename L::TI;
   float2* xa = reinterpret_cast<float2*>(smem_raw);
   float2* xb = xa + LINES * L::XBUF;
   CF* twf = reinterpret_cast<CF*>(xb + LINES * L::XBUF);
@@ -249,10 +249,10 @@ __global__ void __launch_bounds__(LINES * L::R2) line_pass_kernel(float2* __rest
       double s, c;
       const int k1 = i / L::R2, t = i % L::R2;
       sincospi(-2.0 * double((t * k1) % L::N) / L::N, &s, &c);
-      twf[i] = make_c<CF>(c, s);
+      twf[i] = make_tw<CF>(c, s);
       const int nn = i / L::R1, k2 = i % L::R1;
       sincospi(2.0 * double((nn * k2) % L::N) / L::N, &s, &c);
-      twi[i] = make_c<CI>(c, s);
+      twi[i] = make_tw<CI>(c, s);
     }
   }
   __syncthreads();

@@ -106,20 +106,20 @@ __device__ __forceinline__ float block_sum(float v, float* red) {
 
 // Twiddle tables for an N = R1*R2 line, in FP64 rounded once to float.
 template <class L>
-__device__ void fill_twiddles(typename L::CF* twf, typename L::CI* twi) {
+__device__ void fill_twiddles(typename L::TF* twf, typename L::TI* twi) {
   if constexpr (!L::kFft) return;
   for (int i = threadIdx.x; i < L::N; i += blockDim.x) {
     {  // twf[k1*R2 + t] = exp(-2 pi i t k1 / N)
       const int k1 = i / L::R2, t = i % L::R2;
       double s, c;
       sincospi(-2.0 * double((t * k1) % L::N) / L::N, &s, &c);
-      twf[i] = make_c<typename L::CF>(c, s);
+      twf[i] = make_tw<typename L::TF>(c, s);
     }
     {  // twi[n*R1 + k1] = exp(+2 pi i n k1 / N)
       const int nn = i / L::R1, k1 = i % L::R1;
       double s, c;
       sincospi(2.0 * double((nn * k1) % L::N) / L::N, &s, &c);
-      twi[i] = make_c<typename L::CI>(c, s);
+      twi[i] = make_tw<typename L::TI>(c, s);
     }
   }
 }
@@ -177,8 +177,8 @@ __device__ void prefetch_screen(const Params& p, const Item& it, float2* scr_s) 
 
 // One (site, segment, line block) work item.
 template <class L, int LINES>
-__device__ void process(const Params& p, const Item& it, float2* xa, float2* xb, const typename L::CF* twf,
-                        const typename L::CI* twi, float* red, const float2* scr_s) {
+__device__ void process(const Params& p, const Item& it, float2* xa, float2* xb, const typename L::TF* twf,
+                        const typename L::TI* twi, float* red, const float2* scr_s) {
   constexpr int R1 = L::R1, R2 = L::R2;
   const StageP& st = p.st[it.stage];
   const int N = st.size;
@@ -310,13 +310,13 @@ struct Smem {
 };
 
 template <class L, int LINES>
-__global__ void __launch_bounds__(LINES * L::R2, (L::R1 > 16 ? 256 : 512) / (LINES * L::R2)) persistent_kernel(Params p) {
+__global__ void __launch_bounds__(LINES * L::R2, L::kMinBlocks * 128 / (LINES * L::R2)) persistent_kernel(Params p) {
   extern __shared__ float4 smem_raw[];
   float2* xa = reinterpret_cast<float2*>(smem_raw);
   float2* xb = xa;
-  auto* twf = reinterpret_cast<typename L::CF*>(xa + Smem<L, LINES>::xbuf + Smem<L, LINES>::xbuf % 2);
-  auto* twi = reinterpret_cast<typename L::CI*>(reinterpret_cast<char*>(twf) + (L::kFft ? L::N * sizeof(typename L::CF) : 0));
-  float2* scr_s = reinterpret_cast<float2*>(reinterpret_cast<char*>(twi) + (L::kFft ? L::N * sizeof(typename L::CI) : 0));
+  auto* twf = reinterpret_cast<typename L::TF*>(xa + Smem<L, LINES>::xbuf + Smem<L, LINES>::xbuf % 2);
+  auto* twi = reinterpret_cast<typename L::TI*>(reinterpret_cast<char*>(twf) + (L::kFft ? L::N * sizeof(typename L::TF) : 0));
+  float2* scr_s = reinterpret_cast<float2*>(reinterpret_cast<char*>(twi) + (L::kFft ? L::N * sizeof(typename L::TI) : 0));
   float* red = reinterpret_cast<float*>(scr_s + Smem<L, LINES>::screen);
   __shared__ long long s_item;
   __shared__ int s_abort;
@@ -369,13 +369,13 @@ __global__ void __launch_bounds__(LINES * L::R2, (L::R1 > 16 ? 256 : 512) / (LIN
 }
 
 template <class L, int LINES>
-__global__ void __launch_bounds__(LINES * L::R2, (L::R1 > 16 ? 256 : 512) / (LINES * L::R2)) batched_kernel(Params p) {
+__global__ void __launch_bounds__(LINES * L::R2, L::kMinBlocks * 128 / (LINES * L::R2)) batched_kernel(Params p) {
   extern __shared__ float4 smem_raw[];
   float2* xa = reinterpret_cast<float2*>(smem_raw);
   float2* xb = xa;
-  auto* twf = reinterpret_cast<typename L::CF*>(xa + Smem<L, LINES>::xbuf + Smem<L, LINES>::xbuf % 2);
-  auto* twi = reinterpret_cast<typename L::CI*>(reinterpret_cast<char*>(twf) + (L::kFft ? L::N * sizeof(typename L::CF) : 0));
-  float2* scr_s = reinterpret_cast<float2*>(reinterpret_cast<char*>(twi) + (L::kFft ? L::N * sizeof(typename L::CI) : 0));
+  auto* twf = reinterpret_cast<typename L::TF*>(xa + Smem<L, LINES>::xbuf + Smem<L, LINES>::xbuf % 2);
+  auto* twi = reinterpret_cast<typename L::TI*>(reinterpret_cast<char*>(twf) + (L::kFft ? L::N * sizeof(typename L::TF) : 0));
+  float2* scr_s = reinterpret_cast<float2*>(reinterpret_cast<char*>(twi) + (L::kFft ? L::N * sizeof(typename L::TI) : 0));
   float* red = reinterpret_cast<float*>(scr_s + Smem<L, LINES>::screen);
   fill_twiddles<L>(twf, twi);
   __syncthreads();
@@ -477,6 +477,7 @@ int launch_batched_any(Params& p, int stage, int k, int site0, int batch, cudaSt
     case 512:
       if (p.precision == MM_PRECISION_FP64) return launch_batched_fft<double2, double2>(p, stage, k, site0, batch, s);
       if (p.precision == MM_PRECISION_MIXED) return launch_batched_fft<float2, double2>(p, stage, k, site0, batch, s);
+      if (p.precision == MM_PRECISION_COMPENSATED) return launch_batched_fft<cfx, cfx>(p, stage, k, site0, batch, s);
       return launch_batched_fft<float2, float2>(p, stage, k, site0, batch, s);
     default:
       if (n <= 128) return launch_batched<DenseLine<8>, kLinesDense>(p, stage, k, site0, batch, s);
@@ -521,6 +522,7 @@ int launch_persistent_any(Params& p, cudaStream_t s) {
   }
   if (p.precision == MM_PRECISION_FP64) return launch_persistent_fft<double2, double2>(p, s);
   if (p.precision == MM_PRECISION_MIXED) return launch_persistent_fft<float2, double2>(p, s);
+  if (p.precision == MM_PRECISION_COMPENSATED) return launch_persistent_fft<cfx, cfx>(p, s);
   return launch_persistent_fft<float2, float2>(p, s);
 }
 
@@ -590,7 +592,7 @@ int build_params(const mm_stage_plan* plan, int slots, Params& p) {
   p.nsites = plan->nsites;
   p.slots = slots;
   MM_CHECK_ARG(plan->precision == MM_PRECISION_FP32 || plan->precision == MM_PRECISION_FP64 ||
-                   plan->precision == MM_PRECISION_MIXED,
+                   plan->precision == MM_PRECISION_MIXED || plan->precision == MM_PRECISION_COMPENSATED,
                "unknown precision %d", plan->precision);
   p.precision = plan->precision;
   p.blocks_per_site = cum;

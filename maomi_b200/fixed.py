@@ -109,7 +109,7 @@ def assemble(config, out, shape, *, mask_mode="matlab_v4", z_positions=None, cut
 
 
 def stage_device(config, raw_fields, points_um=None, *, uin=None, device="cuda", tails=True, count_per_axis=65,
-                 slots=64, schedule=None, plan=None, check=True, events=None, precision="fp64"):
+                 slots=64, schedule=None, plan=None, check=True, events=None, precision="compensated"):
     """Fused optical stage leaving every product on the device.
 
     Phase preparation (inside ``OpticalPlan``), the persistent propagation of
@@ -213,7 +213,7 @@ def stage_to_host(config, dev, *, return_psf_3d=True, out=None):
 
 
 def run_stage(config, raw_fields, points_um=None, *, uin=None, device="cuda", tails=True, count_per_axis=65,
-              slots=64, schedule=None, return_psf_3d=True, plan=None, check=True, precision="fp64"):
+              slots=64, schedule=None, return_psf_3d=True, plan=None, check=True, precision="compensated"):
     """The whole optical stage on the GPU, returning the host result dictionary
     of maomi.optics.propagate (optics.py:341-381) / fixed.assemble."""
     dev = stage_device(config, raw_fields, points_um, uin=uin, device=device, tails=tails,

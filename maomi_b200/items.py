@@ -60,10 +60,10 @@ def schedule(steps, slots, nblocks):
 class ItemQueue:
     """Device-side uneven workload with one queue per window size."""
 
-    def __init__(self, classes, *, device="cuda", precision="mixed"):
+    def __init__(self, classes, *, device="cuda", precision="compensated"):
         _lib.require_cuda(device)
         if precision not in _lib.PRECISIONS:
-            raise ValueError("precision must be fp32, mixed or fp64")
+            raise ValueError("precision must be one of " + ", ".join(_lib.PRECISIONS))
         self.device, self.precision = device, precision
         self.classes = [c for c in classes if len(c.steps)]
         self.graph = None
@@ -190,7 +190,7 @@ def gaussian_field(n, waist_px):
 
 
 def uneven_workload(count=6000, *, seed=17, device="cuda", wavelength_um=0.92, n_medium=1.35, pitch_um=0.5,
-                    dz_um=1.0, sizes=SIZES, probs=(0.4, 0.3, 0.2, 0.1), depth=(16, 120), precision="mixed",
+                    dz_um=1.0, sizes=SIZES, probs=(0.4, 0.3, 0.2, 0.1), depth=(16, 120), precision="compensated",
                     slots=32):
     """Seeded mixed workload: window sizes drawn from `sizes` with `probs`,
     depths uniform in `depth` (inclusive), per-item refractive-index screens
