@@ -313,6 +313,81 @@ int mm_local_render(const mm_local_desc* desc, const double* source /* (sx,sy,sz
 int mm_gemm_bf16_tn(const void* a, const void* b, float* d, int m, int n, int k, int* err, int check,
                     void* stream);
 
+/* ------------------------------------------------------------------------
+ * Learned PSF surrogate (Fourier neural operator, 4 layers of width 32,
+ * 12 x 12 retained modes, BF16 tensor-core GEMMs with FP32 accumulation).
+ * No reference counterpart: the reference has no learned component.  A
+ * site's input is its 64 x 64 window of 16 pooled screen groups (plus two
+ * coordinate channels); its output the 64 x 64 x 9 focal PSF, unit sum.
+ * All buffers are device memory the caller allocates; BF16 matrices are
+ * row-major.  Shapes for S sites:
+ *   constants  F (576,4096), G (4096,576), FT = F^T, GT = G^T
+ *   params     FP32 flat vector, layout from mm_surrogate_layout; grads same
+ *   wb[l]/wtb[l] (32,32) BF16 copies of W_l and W_l^T; wlb (32,32); wpb (16,32); wptb (32,16)
+ *   base (4096,16) FP32 mean PSF added to the projection
+ *   xp (S*4096,32) / xc (S*32,4096) inputs; hp[l]/hc[l] (l = 0..4) activations, same shapes
+ *   z[l] (S,4096,32) FP32 pre-activations (l = 0..2 needed for backward)
+ *   v[l] (S,576,32) FP32 spectral coefficients; voc (S*32,576) BF16 scratch
+ *   y (S,4096,16) FP32 prediction (planes 0..8 used)
+ *   backward: dyp (S*4096,16), dyc (S*16,4096), dzp[2] (S*4096,32), dzc[2]
+ *   (S*32,4096) BF16; dvo (S,576,32) FP32; dvc (S*32,576) BF16
+ *   err: zeroed device int (bit 1: site off the input grid, bit 4: a
+ *   tensor-core pipeline wait timed out)
+ */
+typedef struct {
+  int sites;
+  const void* F;
+  const void* G;
+  const void* FT;
+  const void* GT;
+  float* params;
+  float* grads;
+  void* wb[4];
+  void* wtb[4];
+  void* wlb;
+  void* wpb;
+  void* wptb;
+  const float* base;
+  const void* xp;
+  const void* xc;
+  void* hp[5];
+  void* hc[5];
+  float* z[4];
+  float* v[4];
+  void* voc;
+  float* y;
+  void* dyp;
+  void* dyc;
+  void* dzp[2];
+  void* dzc[2];
+  float* dvo;
+  void* dvc;
+  int* err;
+} mm_surrogate_desc;
+
+/* Offsets (floats) of Wl, bl, {W_l, b_l, Rr_l, Ri_l} for l = 0..3, Wp, bp and the total (21 entries). */
+int mm_surrogate_layout(long long* offsets, int n);
+/* Fill the BF16 spectral matrices. */
+int mm_surrogate_constants(void* F, void* G, void* FT, void* GT, void* stream);
+/* Prediction y for d->sites sites (refreshes the BF16 weight copies first). */
+int mm_surrogate_forward(const mm_surrogate_desc* d, int check, void* stream);
+/* Loss (mean over sites of ||y - t||^2 / ||t||^2, planes 0..8) and every
+ * parameter gradient into d->grads, after mm_surrogate_forward on the same d.
+ * target: (S,4096,16) FP32. */
+int mm_surrogate_backward(const mm_surrogate_desc* d, const float* target, double* loss, int check, void* stream);
+/* One Adam step (bias-corrected, step >= 1) over n parameters. */
+int mm_surrogate_adam(float* params, const float* grads, float* m, float* v, long long n, float lr, float beta1,
+                      float beta2, float eps, int step, void* stream);
+/* Site inputs from the raw A/B/C fields (each (h, w, z_part) FP32): screens
+ * grouped by groups[0..16] (global screen index ranges), 4x4-pooled into
+ * pooled (16, h/4, w/4), times scale; then each site's 64 x 64 window at
+ * offsets/4 (offsets multiples of 4) into xp / xc. */
+int mm_surrogate_inputs(const float* const* raw, const int* zpart, int h, int w, const int* groups, float scale,
+                        float* pooled, const int* offsets, int sites, void* xp, void* xc, int* err, int check,
+                        void* stream);
+/* y (S,4096,16) -> PSF planes (S,9,64,64), negatives clipped to 0. */
+int mm_surrogate_planes(const float* y, float* out, int sites, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -62,6 +62,18 @@ class LocalDesc(Structure):
                 ("detection", c_int), ("correlate", c_int), ("plane", c_int)]
 
 
+class SurrogateDesc(ctypes.Structure):
+    _fields_ = [("sites", c_int), ("F", c_void_p), ("G", c_void_p), ("FT", c_void_p),
+                ("GT", c_void_p), ("params", c_void_p), ("grads", c_void_p),
+                ("wb", c_void_p * 4), ("wtb", c_void_p * 4), ("wlb", c_void_p),
+                ("wpb", c_void_p), ("wptb", c_void_p), ("base", c_void_p),
+                ("xp", c_void_p), ("xc", c_void_p), ("hp", c_void_p * 5),
+                ("hc", c_void_p * 5), ("z", c_void_p * 4), ("v", c_void_p * 4),
+                ("voc", c_void_p), ("y", c_void_p), ("dyp", c_void_p), ("dyc", c_void_p),
+                ("dzp", c_void_p * 2), ("dzc", c_void_p * 2), ("dvo", c_void_p),
+                ("dvc", c_void_p), ("err", c_void_p)]
+
+
 # name -> (restype, argtypes)
 SIGNATURES = {
     "mm_version": (c_int, []),
@@ -69,6 +81,15 @@ SIGNATURES = {
     "mm_device_supported": (c_int, []),
     "mm_launch_count": (ctypes.c_ulonglong, []),
     "mm_gemm_bf16_tn": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, c_int, c_void_p, c_int, c_void_p]),
+    "mm_surrogate_layout": (c_int, [c_void_p, c_int]),
+    "mm_surrogate_constants": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "mm_surrogate_forward": (c_int, [POINTER(SurrogateDesc), c_int, c_void_p]),
+    "mm_surrogate_backward": (c_int, [POINTER(SurrogateDesc), c_void_p, c_void_p, c_int, c_void_p]),
+    "mm_surrogate_adam": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, ctypes.c_longlong, c_float, c_float, c_float,
+                                  c_float, c_int, c_void_p]),
+    "mm_surrogate_inputs": (c_int, [c_void_p, c_void_p, c_int, c_int, c_void_p, c_float, c_void_p, c_void_p, c_int,
+                                    c_void_p, c_void_p, c_void_p, c_int, c_void_p]),
+    "mm_surrogate_planes": (c_int, [c_void_p, c_void_p, c_int, c_void_p]),
     "mm_gather_screens": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int, c_int, c_int, c_int, c_void_p]),
     "mm_resample_power": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int,
                                   c_int, c_int, c_int, c_int, c_int, c_int, c_int, c_float, c_void_p]),

@@ -34,7 +34,8 @@ struct Tiles {
   int nk;                // wide K blocks of 64 (0: no wide part)
   int a_row_step;        // wide A row of tile (x, y) = x * a_row_step + y * a_row_ystep
   int a_row_ystep;
-  int b_row_step;        // wide B row = y * b_row_step
+  int b_row_step;        // wide B row = y * b_row_step + x * b_row_xstep
+  int b_row_xstep;
   int nsub;              // sub-blocks (0..8)
   int ksub;              // K16 slices of a sub-block (K2 / 16)
   long long sub_site;    // sub-block A2 row = (y * nsub + j) * sub_site + x * 128 + sub_x0
@@ -108,7 +109,7 @@ __global__ void __launch_bounds__(128, 1)
       if (i < t.nk) {
         umma::mbar_arrive_expect_tx(full + s, kATile + S::kBTile);
         umma::tma_load_2d(a, &mapA, full + s, i * kBK, bx * t.a_row_step + by * t.a_row_ystep);
-        umma::tma_load_2d(b, &mapB, full + s, i * kBK, by * t.b_row_step);
+        umma::tma_load_2d(b, &mapB, full + s, i * kBK, by * t.b_row_step + bx * t.b_row_xstep);
       } else {
         const int j = i - t.nk;
         const long long row = (long long)(by * t.nsub + j) * t.sub_site + (long long)bx * kBM + t.sub_x0;
