@@ -58,6 +58,12 @@ def parse():
     ap.add_argument("--sites", type=int, default=SITES, help="profile a subset of the lattice (not a bench line)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--precision", default="compensated", choices=["compensated", "mixed", "fp64", "fp32"])
+    ap.add_argument("--workload", default="stage", choices=["stage", "surrogate", "uneven", "local"],
+                    help="stage: the headline optical stage; surrogate: the learned PSF path with its plain gate; "
+                         "uneven: 6,000 mixed-size items in one graph; local: the local-PSF render")
+    ap.add_argument("--train-sites", type=int, default=20000)
+    ap.add_argument("--epochs", type=int, default=40)
+    ap.add_argument("--items", type=int, default=6000)
     return ap.parse_args()
 
 
@@ -191,10 +197,190 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def _line(metric, value, unit, args, ms, config, **extra):
+    line = {"metric": metric, "value": value, "unit": unit, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "data": "synthetic",
+            "config": config}
+    line.update(extra)
+    print(json.dumps(line), flush=True)
+
+
+def _timed(fn, steps, warmup, stream):
+    """Device time per call (CUDA events on the launching stream, synchronised on both sides)."""
+    import torch
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(steps):
+        fn()
+    b.record(stream)
+    torch.cuda.synchronize()
+    return a.elapsed_time(b) / steps
+
+
+# Tensor-core FLOPs of one site through the surrogate: lifting 2*4096*32*32,
+# per layer spectral 2*576*4096*32 + inverse 2*4096*576*32 + pointwise
+# 2*4096*32*32, projection 2*4096*32*16.
+SURROGATE_FLOPS_PER_SITE = 2 * 4096 * 32 * 32 + 4 * (2 * 2 * 576 * 4096 * 32 + 2 * 4096 * 32 * 32) + 2 * 4096 * 32 * 16
+
+
+def run_surrogate(args):
+    """Learned PSF path on the 4,225 benchmark sites: pooled inputs, FNO
+    inference, 5 % plain re-propagation gate (whole output replaced by the
+    plain PSFs when the gate's relative L2 error exceeds 1 %), against the
+    plain path producing the same PSFs."""
+    import torch
+    from maomi_b200 import surrogate as S
+    from maomi_b200.backends.cuda.batched import OpticalPlan
+    from maomi_b200.fixed import fixed_locations
+    dev = "cuda:0"
+    torch.cuda.set_device(0)
+    stream = torch.cuda.current_stream(dev)
+    cfg, raw = workload()
+    t0 = time.perf_counter()
+    data = S.training_set(cfg, args.train_sites, seeds=[101, 102, 103, 104, 105, 106], device=dev)
+    t_data = time.perf_counter() - t0
+    model = S.PSFSurrogate(device=dev, seed=0, input_scale=data["scale"])
+    t0 = time.perf_counter()
+    hist = model.fit(data, epochs=args.epochs, batch=64, lr=1e-3, lr_final=5e-5)
+    torch.cuda.synchronize()
+    t_train = time.perf_counter() - t0
+    del data
+    raw_dev = [torch.from_numpy(a).to(dev) for a in raw]
+    pts = fixed_locations(cfg)
+    stage = S.SurrogateStage(model, gate_fraction=0.05, tolerance=0.01, seed=0)
+    holder = {}
+
+    def surrogate_step():
+        holder["res"] = stage.run(cfg, raw_dev, pts)
+
+    def plain_step():
+        plan = OpticalPlan(S.surrogate_config(cfg), raw_dev, device=dev)
+        holder["plain"] = S.plain_targets(cfg, raw_dev, pts, device=dev, plan=plan)[0]
+
+    with Clocks(0) as clk:
+        ms = _timed(surrogate_step, args.steps, args.warmup, stream)
+    ms_plain = _timed(plain_step, args.steps, args.warmup, stream)
+    res = holder["res"]
+    ref = S.targets_to_planes(holder["plain"])
+    plan = OpticalPlan(S.surrogate_config(cfg), raw_dev, device=dev)
+    xp, xc, _ = S.site_inputs(raw_dev, plan.offsets(pts)[1], scale=model.input_scale, device=dev)
+    pred = model.predict(xp, xc)
+    err = S.rel_l2_per_site(pred, ref)
+    ms_pred = _timed(lambda: model.predict(xp, xc), args.steps, args.warmup, stream)
+    flops = len(pts) * SURROGATE_FLOPS_PER_SITE
+    pk, pk_kind = peaks()
+    achieved = flops / (ms_pred * 1e-3) / 1e12
+    gate = {k: v for k, v in res["gate"].items() if k != "sites"}
+    gate["sites"] = len(res["gate"]["sites"])
+    _line("surrogate-path sites/s at 512^2x60 (5% plain gate at 1% rel-L2)", len(pts) / (ms * 1e-3), "sites/s", args,
+          ms, {"workload": "4,225 benchmark sites, 64x64x9 focal intensity; FNO 4 layers, width 32, 12x12 modes",
+               "train_sites": args.train_sites, "epochs": args.epochs},
+          dtype="bf16 (tensor cores, FP32 accumulation)", source=res["source"], gate=gate,
+          plain_psf_sites_per_s=len(pts) / (ms_plain * 1e-3), speedup_vs_plain=ms_plain / ms,
+          surrogate_rel_l2={"median": float(err.median()), "max": float(err.max()),
+                            "aggregate": float(S.rel_l2_per_site(pred.reshape(1, -1), ref.reshape(1, -1))[0])},
+          training={"data_s": t_data, "train_s": t_train, "final_loss": hist[-1]},
+          roofline={"bound": "tensor", "achieved": achieved, "peak": pk["bf16_tflops"], "unit": "TFLOP/s",
+                    "frac": achieved / pk["bf16_tflops"], "traffic": None, "kernel": "surrogate inference",
+                    "kernel_ms": ms_pred, "flops_per_launch": flops, "peak_source": pk_kind},
+          clocks=clk.summary())
+
+
+def run_uneven(args):
+    """6,000 mixed-size items (64..512 windows, 16..120 steps) through one
+    CUDA graph of per-size persistent launches, schedule by the autotuner."""
+    import torch
+    from maomi_b200.items import uneven_workload
+    dev = "cuda:0"
+    torch.cuda.set_device(0)
+    stream = torch.cuda.current_stream(dev)
+    q, meta = uneven_workload(args.items, seed=17, device=dev)
+    tuning = q.autotune()
+    q.capture()
+    with Clocks(0) as clk:
+        ms = _timed(q.replay, args.steps, args.warmup, stream)
+    n = meta["sizes"].astype(np.int64)
+    steps = meta["steps"].astype(np.int64)
+    nbytes = int((24 * n * n * steps).sum())
+    pk, pk_kind = peaks()
+    achieved = nbytes / (ms * 1e-3) / 1e9
+    # CPU: the oracle's split-step loop on one item of each size
+    from oracle import optics as O
+    t_cpu, work_cpu = 0.0, 0
+    for size in (64, 128, 256, 512):
+        u0 = np.ones((size, size), np.complex64) / size
+        phi = np.ones((size, size, 8), np.complex64)
+        z = np.arange(9) * 1e-6
+        t0 = time.perf_counter()
+        O.fresnel(u0, np.float32(0.92e-6), np.full(9, 0.5e-6), z, phi, np.float32(1.35))
+        t_cpu += time.perf_counter() - t0
+        work_cpu += 8 * size * size
+    cpu_items = work_cpu / t_cpu / float((n * n * steps).mean())
+    _line("uneven items/s (6,000 mixed 64..512 windows, 16..120 steps, one CUDA graph)", args.items / (ms * 1e-3),
+          "items/s", args, ms, {"workload": f"{args.items} items, sizes p=(.4,.3,.2,.1), depths U(16,120)",
+                                "autotuned": {str(k): v for k, v in tuning.items()}},
+          dtype="c64", e2e=None,
+          roofline={"bound": "hbm", "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
+                    "frac": achieved / pk["hbm_gbs"], "traffic": None, "kernel": "items (persistent, per size)",
+                    "bytes_per_launch": nbytes, "peak_source": pk_kind},
+          cpu_baseline={"value": cpu_items, "unit": "items/s", "cores": 1, "kind": "port",
+                        "sample": "8 split-step slices of one item per size (FP32 oracle), scaled by n^2 * steps"},
+          clocks=clk.summary())
+
+
+def run_local(args):
+    """Local-PSF render of a 256x256x16 somata volume through a 4-depth bank of
+    16x16 local 33x33x9 PSFs (excitation operator, FP64)."""
+    import torch
+    from maomi_b200 import synthetic
+    from maomi_b200.rana import DepthPSFBank, FullFieldPSF, RanaOperator
+    dev = "cuda:0"
+    torch.cuda.set_device(0)
+    stream = torch.cuda.current_stream(dev)
+    vol = synthetic.somata_volume((256, 256, 16), count=400, seed=3)
+    kern = synthetic.psf_bank_kernels(nodes=(16, 16), kernel=(33, 33, 9), depths=4, seed=5).astype(np.float64)
+    xs = ys = np.linspace(0, 256, 16)
+    depths = np.linspace(0, 16, 4)
+    fields = tuple(FullFieldPSF(kern[i], xs, ys, (1., 1., 1.), 920., "excitation") for i in range(4))
+    R = RanaOperator(DepthPSFBank(depths, fields), device=dev)
+    a = vol.astype(np.float64)
+    src = R._backend.array(a)
+    z = (np.arange(16) + .5)
+    wz = R._depth_weights(z)
+    out = R._backend.zeros(a.shape)
+
+    def render():
+        out.zero_()
+        for f, w in zip(R.fields, wz):
+            if np.any(w):
+                R._plan(a.shape, f.kernels, False)(src, zweight=w, out=out)
+
+    with Clocks(0) as clk:
+        ms = _timed(render, args.steps, args.warmup, stream)
+    e2e_ms = _timed(lambda: R.static(vol), args.steps, 1, stream)
+    voxels = vol.size
+    from oracle import local_fft as L
+    t0 = time.perf_counter()
+    L.static([kern[0]], xs, ys, (1., 1., 1.), vol, operator="excitation")
+    t_cpu = (time.perf_counter() - t0) * 4  # four depth kernels
+    _line("local-PSF render voxels/s (256x256x16, 16x16x4 bank of 33x33x9 PSFs)", voxels / (ms * 1e-3), "voxels/s",
+          args, ms, {"workload": "RanaOperator.static, excitation, 400 somata"}, dtype="f64",
+          e2e={"value": voxels / (e2e_ms * 1e-3), "unit": "voxels/s", "h2d_bytes_per_step": int(a.nbytes),
+               "d2h_bytes_per_step": int(a.nbytes)},
+          cpu_baseline={"value": voxels / t_cpu, "unit": "voxels/s", "cores": os.cpu_count() or 1, "kind": "port",
+                        "sample": "one depth kernel of the FP64 SciPy restatement of LocalFFTPlan, times 4"},
+          clocks=clk.summary())
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload != "stage":
+        return {"surrogate": run_surrogate, "uneven": run_uneven, "local": run_local}[args.workload](args)
     import torch
     import torch.distributed as dist
     world = int(os.environ.get("WORLD_SIZE", "1"))
