@@ -61,6 +61,8 @@ def parse():
     ap.add_argument("--workload", default="stage", choices=["stage", "surrogate", "uneven", "local"],
                     help="stage: the headline optical stage; surrogate: the learned PSF path with its plain gate; "
                          "uneven: 6,000 mixed-size items in one graph; local: the local-PSF render")
+    ap.add_argument("--reserve-sms", type=int, default=None,
+                    help="SMs the propagation leaves to the overlapped v4 factorisation (default: the library's)")
     ap.add_argument("--train-sites", type=int, default=20000)
     ap.add_argument("--epochs", type=int, default=40)
     ap.add_argument("--items", type=int, default=6000)
@@ -403,8 +405,9 @@ def main():
     points = fixed_locations(cfg)[:args.sites]
 
     def step(inputs, events=None):
+        extra = {} if args.reserve_sms is None else {"reserve_sms": args.reserve_sms}
         return stage_device(cfg, inputs, points, device=dev, slots=args.slots, schedule=args.schedule, check=False,
-                            events=events, precision=args.precision)
+                            events=events, precision=args.precision, **extra)
 
     # ---- device-resident timing
     for _ in range(args.warmup):
@@ -430,7 +433,7 @@ def main():
     if args.no_e2e:
         if rank == 0:
             print(json.dumps({"profile_case": True, "sites": len(points), "ms_per_step": ms, "kernel_ms": kernel_ms,
-                              "schedule": args.schedule, "slots": args.slots}))
+                              "schedule": args.schedule, "slots": args.slots, "reserve_sms": args.reserve_sms}))
         return
     # ---- end to end through the public API with host buffers
     probe = step(raw_dev)

@@ -76,6 +76,35 @@ int mm_green_apply(const double* points /* (n,2) */, const double* coef /* (n,nc
  * (the matrix solved in maomi/numerics.py:122-129). */
 int mm_green_matrix(const double* points /* (n,2) */, double* G /* (n,n) */, int n, void* stream);
 
+/* mm_green_apply_grid for points at integer coordinates in
+ * [px_min, px_max] x [py_min, py_max]: every query-point offset is a half
+ * integer, so g is tabulated once per offset into `table`
+ * ((X - px_min + px_max) * (Y - py_min + py_max) doubles) and the sums read it;
+ * same point order and FMA chain as mm_green_apply_grid (identical results). */
+int mm_green_apply_grid_table(const double* points, const double* coef, double* out, int n, int X, int Y, int ncoef,
+                              int px_min, int px_max, int py_min, int py_max, double* table, size_t table_bytes,
+                              void* stream);
+
+/* The v4 system of points on a full nx x ny lattice symmetric under both
+ * axis reflections (the fixed site lattice, maomi/fixed.py:15-33) in the basis
+ * of even/odd reflection pairs: four independent symmetric blocks, parity
+ * b = 2*(x odd) + (y odd), each padded to m x m with the identity
+ * (m >= ceil(nx/2)*ceil(ny/2)).  lattice[i*ny + j] = index of the point at
+ * the i-th x and j-th y coordinate.  Same linear system as mm_green_matrix. */
+int mm_green_blocks(const double* points, const int32_t* lattice, int nx, int ny, int m,
+                    double* blocks /* (4,m,m) */, void* stream);
+/* In-place x <- A^-1 x for `batch` column-major m x m LU factorisations (unit
+ * lower L, U, 1-based LAPACK pivots, as from getrf) with nrhs right-hand
+ * sides each (x: (batch, m, nrhs)); one CTA per system (the parity blocks of
+ * the v4 solve). */
+int mm_lu_solve_batched(const double* lu, const int32_t* pivots, int batch, int m, int nrhs, double* x, void* stream);
+
+/* Parity transform of v4 right-hand sides / solutions: inverse = 0 maps
+ * values (n,ncoef) to block components (4,m,ncoef); inverse = 1 maps block
+ * solutions (4,m,ncoef) back to coefficients (n,ncoef). */
+int mm_v4_parity(const int32_t* lattice, int nx, int ny, int m, int ncoef, int inverse, const double* in,
+                 double* out, void* stream);
+
 /* v4 evaluation on a regular pixel grid (queries (i+0.5, j+0.5), i<X, j<Y),
  * the mask-assembly case of maomi/fixed.py:141-144; out is (X,Y,ncoef). */
 int mm_green_apply_grid(const double* points, const double* coef, double* out,
@@ -181,6 +210,10 @@ typedef struct {
                               (FP32 butterflies, every DFT rotation and twiddle
                               constant carried as a hi + lo pair of floats); the
                               field is stored complex64 in every mode             */
+  int reserve_sms;         /* persistent schedule: CTAs that start on SM ids below
+                              this count leave at once, so work queued on other
+                              streams (e.g. the v4 factorisation) runs there
+                              while the sites propagate; 0 = use every SM         */
 } mm_stage_plan;
 
 enum { MM_PRECISION_FP32 = 0, MM_PRECISION_FP64 = 1, MM_PRECISION_MIXED = 2, MM_PRECISION_COMPENSATED = 3 };

@@ -33,7 +33,7 @@ class StagePlan(Structure):
                 ("cut", c_int), ("focal_x0", c_int), ("focal_y0", c_int), ("focal_h", c_int), ("focal_w", c_int),
                 ("tail_weight", c_void_p * 2), ("focal", c_void_p), ("tail_image", c_void_p * 2),
                 ("tail_per_site", c_int), ("tail_profile", c_void_p * 2), ("offsets", c_void_p), ("nsites", c_int),
-                ("precision", c_int)]
+                ("precision", c_int), ("reserve_sms", c_int)]
 
 
 class ItemClass(Structure):
@@ -96,6 +96,11 @@ SIGNATURES = {
     "mm_green_apply": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int, c_int, c_void_p]),
     "mm_green_matrix": (c_int, [c_void_p, c_void_p, c_int, c_void_p]),
     "mm_green_apply_grid": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, c_int, c_int, c_void_p]),
+    "mm_green_blocks": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_void_p, c_void_p]),
+    "mm_lu_solve_batched": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_void_p, c_void_p]),
+    "mm_green_apply_grid_table": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, c_int, c_int, c_int, c_int,
+                                          c_int, c_int, c_void_p, c_size_t, c_void_p]),
+    "mm_v4_parity": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p]),
     "mm_phase_prepare": (c_int, [c_void_p, c_int, c_int, c_int, c_void_p, c_void_p, c_int, c_int, c_void_p, c_void_p,
                                  c_int, c_int, c_float, c_void_p, c_void_p, c_void_p]),
     "mm_pupil": (c_int, [POINTER(PupilDesc), c_void_p, c_void_p, c_void_p]),
@@ -174,6 +179,16 @@ def ptr(t):
     if t is None:
         return None
     return c_void_p(t.data_ptr())
+
+
+def upload(values, device, dtype=None):
+    """Host array -> device tensor through pinned memory on the current
+    stream, without blocking the host (no pipeline drain)."""
+    import torch
+    t = torch.as_tensor(np.ascontiguousarray(values))
+    if dtype is not None:
+        t = t.to(dtype)
+    return t.pin_memory().to(device, non_blocking=True)
 
 
 def stream_of(device=None):

@@ -58,12 +58,38 @@ class ResampleTables:
         mx, my = resample_matrix(h, ss), resample_matrix(w, ss)
         (ix, wx), (iy, wy) = sparse_rows(mx), sparse_rows(my)
         self.shape = (mx.shape[0], my.shape[0])
-        self.ix = torch.as_tensor(ix, device=device)
-        self.wx = torch.as_tensor(wx, device=device)
-        self.iy = torch.as_tensor(iy, device=device)
-        self.wy = torch.as_tensor(wy, device=device)
-        self.mx = torch.as_tensor(mx, dtype=torch.float32, device=device)
-        self.my = torch.as_tensor(my, dtype=torch.float32, device=device)
+        self.ix = _lib.upload(ix, device)
+        self.wx = _lib.upload(wx, device)
+        self.iy = _lib.upload(iy, device)
+        self.wy = _lib.upload(wy, device)
+        self.mx = _lib.upload(mx, device, torch.float32)
+        self.my = _lib.upload(my, device, torch.float32)
+
+
+def _tables(config, g, raw_fields, device):
+    """Device tables that depend on the configuration only: edge windows,
+    transfer kernels, axial weights and the resample operators."""
+    import torch
+    counts = tuple(int(np.shape(a)[-1]) for a in raw_fields)
+    r, ss = config.vres, config.ss
+    n, n2 = g.n, g.n2
+    a, b, c = counts
+    t = {"edges": {k: _lib.upload(edge_window_1d(k), device) for k in {n, n2}}}
+    t["axial"] = {key_: np.asarray(axial_profile(config, size, key_), np.float32)
+                  for key_, size in [("focus", b), ("top", a + 1 - g.cut), ("bottom", c + 1)]}
+    t["kernels"] = [_lib.upload(transfer_kernels(z, size, g.d2, g.wvl, g.nr), device)
+                    for size, z in zip((n, n2, n), g.z)]
+    axial = [t["axial"][k] for k in ("top", "bottom")]
+    t["tail_weight"] = [_lib.upload((trapezoid(len(x)) * x).astype(np.float32), device) for x in axial]
+    t["tail_axial"] = [_lib.upload(x.astype(np.float64) * ss ** 2, device) for x in axial]
+    t["tail_trapezoid"] = [_lib.upload(trapezoid(len(x)), device) for x in axial]
+    t["axial_focus"] = _lib.upload(t["axial"]["focus"], device)
+    fshape = g.focal_shape
+    t["focal_shape"] = (int(fshape[0]), int(fshape[1]))
+    t["focal_resample"] = ResampleTables(*t["focal_shape"], ss, device)
+    t["tail_resample"] = ResampleTables(n2, n2, ss, device)
+    t["scale"] = float(ss ** 4 * (r * (1e6 * g.wvl) ** 1.5) / (np.pi * g.nr))
+    return t
 
 
 class OpticalPlan:
@@ -74,9 +100,10 @@ class OpticalPlan:
         _lib.require_cuda(device)
         if precision not in _lib.PRECISIONS:
             raise ValueError("precision must be one of " + ", ".join(_lib.PRECISIONS))
-        #: arithmetic of the radix-2 line transforms: "fp64" (FP64 butterflies,
-        #: twiddles and filter), "mixed" (forward FP32, inverse FP64) or "fp32";
-        #: fields are stored complex64 in every mode
+        #: arithmetic of the radix-2 line transforms: "compensated" (FP32
+        #: butterflies, rotation and twiddle constants as hi + lo float pairs),
+        #: "fp64" (FP64 butterflies, twiddles and filter), "mixed" (forward
+        #: FP32, inverse FP64) or "fp32"; fields are stored complex64 in every mode
         self.precision = precision
         self.config = copy.deepcopy(config)
         self.device = device
@@ -96,7 +123,8 @@ class OpticalPlan:
         if tuple(u.shape) != (self.n, self.n):
             raise ValueError(f"Input pupil must be {self.n}x{self.n}, got {tuple(u.shape)}")
         stream = _lib.stream_of(device)
-        self.edges = {k: torch.as_tensor(edge_window_1d(k), device=device) for k in {self.n, self.n2}}
+        t = _tables(config, g, raw_fields, device)
+        self.edges = t["edges"]
         # ---- base field: pupil -> tissue top, scaled Fresnel step (FP64 chirps)
         z1 = float(np.float32(g.fl - (config.depth_um + config.volume_um[2] / 2) * 1e-6))
         self.base = torch.empty((self.n, self.n), dtype=torch.complex64, device=device)
@@ -109,21 +137,18 @@ class OpticalPlan:
         # ---- phase screens (Z, H, W) complex64
         scale = config.n_diff * 2 * np.pi / (config.wavelength_um * r)
         self.phases = [self._screens(a, ss, scale) for a in raw_fields]
-        a, b, c = [int(np.shape(x)[-1]) for x in raw_fields]
         self.z_positions = g.z
         self.cut = g.cut
-        self.axial = {key: np.asarray(axial_profile(config, size, key), np.float32)
-                      for key, size in [("focus", b), ("top", a + 1 - self.cut), ("bottom", c + 1)]}
-        self.kernels = [torch.as_tensor(transfer_kernels(z, size, g.d2, g.wvl, g.nr), device=device)
-                        for size, z in zip((self.n, self.n2, self.n), self.z_positions)]
-        self.tail_weight = [torch.as_tensor((trapezoid(len(self.axial[k])) * self.axial[k]).astype(np.float32),
-                                            device=device) for k in ("top", "bottom")]
-        self.axial_focus = torch.as_tensor(self.axial["focus"], device=device)
-        fshape = g.focal_shape
-        self.focal_shape = (int(fshape[0]), int(fshape[1]))
-        self.focal_resample = ResampleTables(*self.focal_shape, ss, device)
-        self.tail_resample = ResampleTables(self.n2, self.n2, ss, device)
-        self.scale = float(ss ** 4 * (r * (1e6 * g.wvl) ** 1.5) / (np.pi * g.nr))
+        self.axial = t["axial"]
+        self.kernels = t["kernels"]
+        self.tail_weight = t["tail_weight"]
+        self.tail_axial = t["tail_axial"]
+        self.tail_trapezoid = t["tail_trapezoid"]
+        self.axial_focus = t["axial_focus"]
+        self.focal_shape = t["focal_shape"]
+        self.focal_resample = t["focal_resample"]
+        self.tail_resample = t["tail_resample"]
+        self.scale = t["scale"]
         self.cache = {}
         self.paths_evaluated = 0
         self.graphs = {}
@@ -143,7 +168,7 @@ class OpticalPlan:
             _lib.call("mm_phase_prepare", _lib.ptr(a), H, W, Z, None, None, Ho, 1, None, None, Wo, 1,
                       float(np.float32(scale)), _lib.ptr(out), None, stream)
             return out
-        t = [torch.as_tensor(x, device=self.device) for x in
+        t = [_lib.upload(x, self.device) for x in
              (ix.astype(np.int32), wx.astype(np.float32), iy.astype(np.int32), wy.astype(np.float32))]
         tmp = torch.empty((Ho, W, Z), dtype=torch.float32, device=self.device)
         _lib.call("mm_phase_prepare", _lib.ptr(a), H, W, Z, _lib.ptr(t[0]), _lib.ptr(t[1]), Ho, ix.shape[1],
@@ -168,12 +193,12 @@ class OpticalPlan:
         return _lib.MM_SCHEDULE_PERSISTENT if schedule == "persistent" else _lib.MM_SCHEDULE_BATCHED
 
     # ------------------------------------------------------------ propagation
-    def run_sites(self, offsets, *, tail_per_site, slots, schedule=None, check=True, events=None):
+    def run_sites(self, offsets, *, tail_per_site, slots, schedule=None, check=True, events=None, reserve_sms=0):
         """Propagate every site; returns device buffers (focal, tail images, profiles)."""
         import torch
         dev = self.device
         P = len(offsets)
-        off = torch.as_tensor(np.ascontiguousarray(offsets, np.int32), device=dev)
+        off = _lib.upload(np.asarray(offsets, np.int32), dev)
         zb = self.kernels[1].shape[0]
         fh, fw = self.focal_shape
         focal = torch.empty((P, zb, fh, fw), dtype=torch.float32, device=dev)
@@ -206,6 +231,7 @@ class OpticalPlan:
         plan.offsets = off.data_ptr()
         plan.nsites = P
         plan.precision = _lib.PRECISIONS[self.precision]
+        plan.reserve_sms = int(reserve_sms)
         lib = _lib.load()
         wbytes = lib.mm_propagate_workspace_size(plan, slots, sched)
         work = torch.empty(wbytes + 256, dtype=torch.uint8, device=dev)

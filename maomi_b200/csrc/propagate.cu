@@ -59,6 +59,7 @@ struct Params {
   // batched schedule: the stage / segment and first site of this launch
   int b_stage, b_k, b_site0;
   int precision;  // MM_PRECISION_*: arithmetic of the radix-2 line transforms
+  int reserve_sms;  // persistent CTAs starting on SM ids below this leave at once
 };
 
 constexpr long long kSpinLimit = 1ll << 24;  // ~ seconds with the backoff below
@@ -320,6 +321,11 @@ __global__ void __launch_bounds__(LINES * L::R2, L::kMinBlocks * 128 / (LINES * 
   float* red = reinterpret_cast<float*>(scr_s + Smem<L, LINES>::screen);
   __shared__ long long s_item;
   __shared__ int s_abort;
+  if (p.reserve_sms > 0) {
+    unsigned sm;
+    asm volatile("mov.u32 %0, %%smid;" : "=r"(sm));
+    if (sm < unsigned(p.reserve_sms)) return;  // uniform per CTA; no item claimed yet
+  }
   fill_twiddles<L>(twf, twi);
   if (threadIdx.x == 0) s_item = (long long)atomicAdd(p.head, 1u);
   __syncthreads();
@@ -595,6 +601,8 @@ int build_params(const mm_stage_plan* plan, int slots, Params& p) {
                    plan->precision == MM_PRECISION_MIXED || plan->precision == MM_PRECISION_COMPENSATED,
                "unknown precision %d", plan->precision);
   p.precision = plan->precision;
+  MM_CHECK_ARG(plan->reserve_sms >= 0 && plan->reserve_sms <= 64, "reserve_sms %d outside 0..64", plan->reserve_sms);
+  p.reserve_sms = plan->reserve_sms;
   p.blocks_per_site = cum;
   return MM_OK;
 }

@@ -40,17 +40,20 @@ __global__ void resample_power_kernel(const float2* __restrict__ field, const in
 }
 
 // One CTA per (site, output row x): psf[p,x,:,:] (Y*Z values, z fastest).
+// Inputs are read plane by plane with y fastest (coalesced rows of the focal
+// crops), staged in shared memory and written out with z fastest.
 __global__ void focal_finalize_kernel(const float* __restrict__ focal, const int* __restrict__ ix,
                                       const float* __restrict__ wx, int KX, const int* __restrict__ iy,
                                       const float* __restrict__ wy, int KY, const float* __restrict__ axial,
                                       float scale, int Z, int H, int W, int X, int Y, float* __restrict__ psf,
                                       double* __restrict__ energies) {
+  extern __shared__ float tile[];  // Y x (Z + 1)
   __shared__ double red[32];
   const int p = blockIdx.y, x = blockIdx.x;
   const float* src = focal + (size_t)p * Z * H * W;
   double acc = 0.0;
   for (int o = threadIdx.x; o < Y * Z; o += blockDim.x) {
-    const int y = o / Z, z = o % Z;
+    const int z = o / Y, y = o % Y;
     const float* plane = src + (size_t)z * H * W;
     float value = 0.f;
     for (int i = 0; i < KX; ++i) {
@@ -66,8 +69,13 @@ __global__ void focal_finalize_kernel(const float* __restrict__ focal, const int
       value += a * row;
     }
     const float v = scale * value * __ldg(axial + z);
-    if (psf) psf[(((size_t)p * X + x) * Y) * Z + o] = v;
+    tile[y * (Z + 1) + z] = v;
     acc += v;
+  }
+  __syncthreads();
+  if (psf) {
+    float* dst = psf + ((size_t)p * X + x) * Y * Z;
+    for (int o = threadIdx.x; o < Y * Z; o += blockDim.x) dst[o] = tile[(o / Z) * (Z + 1) + o % Z];
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
@@ -179,8 +187,13 @@ extern "C" int mm_focal_finalize(const float* focal, const int32_t* ix, const fl
   MM_CHECK_ARG(P >= 1 && Z >= 1 && H >= 1 && W >= 1 && X >= 1 && Y >= 1 && P <= 65535, "bad focal sizes");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   MM_CHECK_CUDA(cudaMemsetAsync(energies, 0, sizeof(double) * P, s), "zero energies");
-  focal_finalize_kernel<<<dim3(X, P), 128, 0, s>>>(focal, ix, wx, KX, iy, wy, KY, axial, scale, Z, H, W, X, Y, psf,
-                                                   energies);
+  const size_t tile = sizeof(float) * (size_t)Y * (Z + 1);
+  MM_CHECK_ARG(tile <= 200 * 1024, "focal crop %d x %d planes too large for one tile", Y, Z);
+  if (tile > 48 * 1024)
+    MM_CHECK_CUDA(cudaFuncSetAttribute(focal_finalize_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tile),
+                  "cudaFuncSetAttribute(focal finalize)");
+  focal_finalize_kernel<<<dim3(X, P), 256, tile, s>>>(focal, ix, wx, KX, iy, wy, KY, axial, scale, Z, H, W, X, Y, psf,
+                                                      energies);
   MM_CHECK_LAUNCH("focal finalize");
   if (psf_sum && psf_abs_sum && psf) {
     const long long E = (long long)X * Y * Z;

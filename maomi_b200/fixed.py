@@ -15,7 +15,7 @@ import numpy as np
 
 from . import _lib
 from ._optical_math import gaussian_beam_size
-from .numerics import v4_coefficients_device, v4_evaluate_grid_device, v4_interpolate
+from .numerics import v4_evaluate_grid_device, v4_factor_device, v4_interpolate, v4_solve_device
 
 
 def fixed_locations(config, count_per_axis=65):
@@ -51,6 +51,19 @@ def field_shapes(config):
     return [(int(xy[0] + n), int(xy[1] + n), int(np.ceil(za / pc))),
             (int(xy[0] + n2), int(xy[1] + n2), zb),
             (int(xy[0] + n), int(xy[1] + n), int(np.ceil(nc / pc)))]
+
+
+_SIDE_STREAMS = {}
+RESERVE_SMS = 0   # SMs the persistent kernel leaves to the overlapped v4 factorisation
+
+
+def _side_stream(device):
+    """A high-priority stream per device for work that overlaps the propagation."""
+    import torch
+    key = str(torch.device(device))
+    if key not in _SIDE_STREAMS:
+        _SIDE_STREAMS[key] = torch.cuda.Stream(device=device, priority=-1)
+    return _SIDE_STREAMS[key]
 
 
 def _psf_z(config, z, profile):
@@ -109,7 +122,8 @@ def assemble(config, out, shape, *, mask_mode="matlab_v4", z_positions=None, cut
 
 
 def stage_device(config, raw_fields, points_um=None, *, uin=None, device="cuda", tails=True, count_per_axis=65,
-                 slots=64, schedule=None, plan=None, check=True, events=None, precision="compensated"):
+                 slots=64, schedule=None, plan=None, check=True, events=None, precision="compensated",
+                 reserve_sms=RESERVE_SMS):
     """Fused optical stage leaving every product on the device.
 
     Phase preparation (inside ``OpticalPlan``), the persistent propagation of
@@ -117,30 +131,45 @@ def stage_device(config, raw_fields, points_um=None, *, uin=None, device="cuda",
     FP64 site sums and the FP64 v4 mask assembly.  Returns a dict of device
     tensors (``psf_3d``, ``energies``, ``psf_sum``, ``psf_abs_sum``, ``masks``,
     tail ``profiles``/``weights``/``convmask``) plus the plan.  ``events``
-    (a pair of CUDA events) brackets the propagation launch."""
+    (a pair of CUDA events) brackets the propagation launch.  The v4 system
+    depends on the site positions only; it is factored on a high-priority side
+    stream first, so it runs while the host prepares the plan (and on the
+    ``reserve_sms`` SMs the persistent kernel can leave to it)."""
     import torch
     from .backends.cuda.batched import OpticalPlan, trapezoid
     _lib.require_cuda(device)
-    if plan is None:
-        plan = OpticalPlan(config, raw_fields, uin=uin, device=device, precision=precision)
     points = fixed_locations(config, count_per_axis) if points_um is None else np.asarray(points_um, float)
-    pts, off = plan.offsets(points)
-    P = len(pts)
-    dev = plan.device
+    if np.any(points < 0) or np.any(points > np.asarray(config.volume_um[:2])):
+        raise ValueError("Outside FOV")
+    dev = device if plan is None else plan.device
     with torch.inference_mode():
-        res = plan.run_sites(off, tail_per_site=False, slots=slots, schedule=schedule, check=check, events=events)
+        main = torch.cuda.current_stream(dev)
+        factor = None
+        if len(points) > 1:
+            side = _side_stream(dev)
+            side.wait_stream(main)
+            with torch.cuda.stream(side):
+                factor = v4_factor_device(points * config.vres, device=dev)
+        if plan is None:
+            plan = OpticalPlan(config, raw_fields, uin=uin, device=device, precision=precision)
+        pts, off = plan.offsets(points)
+        P = len(pts)
+        res = plan.run_sites(off, tail_per_site=False, slots=slots, schedule=schedule, check=check, events=events,
+                             reserve_sms=reserve_sms if factor is not None else 0)
         psf, energies, s1, s2 = plan.finalize_focal(res["focal"], psf=True, sums=True)
         prof, wts = [], []
         for j in range(2):
-            axial = plan.axial["top" if j == 0 else "bottom"].astype(np.float64)
-            pj = res["profiles"][j] * torch.as_tensor(axial * config.ss ** 2, device=dev)
+            pj = res["profiles"][j] * plan.tail_axial[j]
             prof.append(pj)
-            wts.append((pj * torch.as_tensor(trapezoid(len(axial)), device=dev)).sum(1) * config.prop_um)
+            wts.append((pj * plan.tail_trapezoid[j]).sum(1) * config.prop_um)
         values = torch.stack([energies, wts[0], wts[1]] if tails else [energies], 1)
         shape = tuple(int(v) for v in np.round(np.array(config.volume_um[:2]) * config.vres))
         if P > 1:
-            p_dev, coef = v4_coefficients_device(pts * config.vres, values, device=dev)
-            masks = v4_evaluate_grid_device(p_dev, coef, *shape, device=dev)
+            main.wait_stream(side)
+            for t in factor.tensors():
+                t.record_stream(main)
+            p_dev, coef = v4_solve_device(factor, values)
+            masks = v4_evaluate_grid_device(p_dev, coef, *shape, device=dev, points_host=pts * config.vres)
         else:
             masks = values[0].reshape(1, 1, -1).expand(shape[0], shape[1], -1).contiguous()
         convs = []

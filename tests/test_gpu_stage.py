@@ -199,3 +199,26 @@ def test_full_size_translation_invariance():
     for t in ("psfT", "psfB"):
         assert out[t]["weight"] > 0
         np.testing.assert_allclose(out[t]["weights_per_point"], out[t]["weights_per_point"][0], rtol=1e-6)
+
+
+@pytest.mark.gpu
+def test_v4_lattice_parity_solve_matches_dense():
+    """The fixed 65x65 site lattice solved as four reflection-parity blocks
+    gives the dense FP64 LU's masks (4,225 points -> 512x512, 3 columns)."""
+    from maomi_b200 import synthetic
+    from maomi_b200.fixed import fixed_locations
+    from maomi_b200.numerics import lattice_index, v4_evaluate_grid_device, v4_factor_device, v4_solve_device
+    from maomi_b200.optics import OpticalConfig
+    cfg = synthetic.benchmark_stage_config(OpticalConfig)
+    pts = fixed_locations(cfg) * cfg.vres
+    assert lattice_index(pts) is not None
+    vals = np.random.default_rng(3).uniform(0.5, 2.0, (len(pts), 3))
+    p, c_lat = v4_solve_device(v4_factor_device(pts), vals)
+    _, c_den = v4_solve_device(v4_factor_device(pts, structured=False), vals)
+    m_lat = v4_evaluate_grid_device(p, c_lat, 512, 512).cpu().numpy()
+    m_den = v4_evaluate_grid_device(p, c_den, 512, 512).cpu().numpy()
+    assert rel_l2(m_lat, m_den) < 1e-9
+    # tabulated Green function on the integer lattice: the same sums, bit for bit
+    m_tab = v4_evaluate_grid_device(p, c_lat, 512, 512, points_host=pts).cpu().numpy()
+    np.testing.assert_array_equal(m_tab, m_lat)
+    assert rel_l2(c_lat.cpu().numpy(), c_den.cpu().numpy()) < 1e-6

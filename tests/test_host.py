@@ -166,3 +166,19 @@ def test_product_refuses_cpu():
         run_fixed(cfg, raw_fields=[np.zeros((3, 3, 3), np.float32)] * 3)
     with pytest.raises(ValueError):
         run_fixed(cfg, raw_fields=None)
+
+
+def test_lattice_index_detects_symmetric_lattices():
+    from maomi_b200.numerics import lattice_index
+    xs, ys = np.arange(5) * 8.0, np.arange(4) * 8.0 + 2.0
+    pts = np.array([(x, y) for x in xs for y in ys])
+    perm = np.random.default_rng(0).permutation(len(pts))
+    nx, ny, idx = lattice_index(pts[perm])
+    assert (nx, ny) == (5, 4)
+    np.testing.assert_array_equal(pts[perm][idx], pts)
+    assert lattice_index(pts[:-1]) is None                       # incomplete
+    bent = pts.copy()
+    bent[pts[:, 0] == 32.0, 0] = 33.0                            # not symmetric
+    assert lattice_index(bent) is None
+    assert lattice_index(np.array([[0.0, 0.0], [1.0, 0.0]])) is None  # one row
+
