@@ -394,7 +394,7 @@ def main():
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device(dev))
     from maomi_b200 import _lib
-    from maomi_b200.fixed import stage_device, stage_to_host
+    from maomi_b200.fixed import stage_device
     lib = _lib.load()
     cfg, raw = workload(rank)
     raw_pinned = [torch.from_numpy(a).pin_memory() for a in raw]
@@ -435,26 +435,31 @@ def main():
             print(json.dumps({"profile_case": True, "sites": len(points), "ms_per_step": ms, "kernel_ms": kernel_ms,
                               "schedule": args.schedule, "slots": args.slots, "reserve_sms": args.reserve_sms}))
         return
-    # ---- end to end through the public API with host buffers
-    probe = step(raw_dev)
-    pinned = {k: torch.empty(v.shape, dtype=v.dtype, pin_memory=True) for k, v in
-              (("masks", probe["masks"]), ("psf_3d", probe["psf_3d"]))}
+    # ---- end to end through the public API with host buffers: run_stages
+    # uploads each block's raw fields from pinned host memory and copies every
+    # product back to pinned host memory; block i+1 computes while block i's
+    # products are copied (all copies inside the timed region)
+    from maomi_b200.fixed import run_stages
+    kw = {"slots": args.slots, "schedule": args.schedule, "check": False, "precision": args.precision,
+          "reuse": True}
+    if args.reserve_sms is not None:
+        kw["reserve_sms"] = args.reserve_sms
+    for _ in run_stages(cfg, [raw_pinned] * 3, points, device=dev, **kw):
+        pass
     h2d = sum(a.numel() * a.element_size() for a in raw_pinned)
-    d2h = sum(v.numel() * v.element_size() for v in pinned.values())
     e_start, e_stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize(dev)
     e_start.record(stream)
-    for _ in range(args.steps):
-        inputs = [a.to(dev, non_blocking=True) for a in raw_pinned]
-        res = stage_to_host(cfg, step(inputs), out=pinned)
+    for res in run_stages(cfg, [raw_pinned] * args.steps, points, device=dev, **kw):
+        pass
     e_stop.record(stream)
     torch.cuda.synchronize(dev)
     e2e_ms = e_start.elapsed_time(e_stop) / args.steps
-    d2h += sum(np.asarray(res[k]).nbytes for k in ("psf", "psf_raw", "energies")) + sum(
+    d2h = sum(np.asarray(res[k]).nbytes for k in ("psf_3d", "mask_raw", "psf", "psf_raw", "energies")) + sum(
         np.asarray(res[t][k]).nbytes for t in ("psfT", "psfB") for k in ("convmask", "weights_per_point",
-                                                                          "profiles_per_point"))
+                                                                          "profiles_per_point", "mask_raw"))
     times = torch.tensor([ms, e2e_ms, kernel_ms], dtype=torch.float64, device=dev)
     if world > 1:
         dist.all_reduce(times, op=dist.ReduceOp.MAX)

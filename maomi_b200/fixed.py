@@ -188,57 +188,131 @@ def stage_device(config, raw_fields, points_um=None, *, uin=None, device="cuda",
                 profiles=prof, weights=wts, convmask=convs, tails=bool(tails))
 
 
-def stage_to_host(config, dev, *, return_psf_3d=True, out=None):
-    """Host result dictionary (the keys of maomi.optics.propagate / assemble)
-    from ``stage_device`` output.  ``out`` may hold pinned host buffers."""
+def stage_copy_async(dev, *, return_psf_3d=True, out=None, stream=None):
+    """Enqueue the device -> host copies of one ``stage_device`` result on
+    ``stream`` (ordered after the current stream's work); returns the pending
+    copy for ``stage_result``.  Destinations are pinned host buffers (``out``
+    entries where given), so the copies overlap later device work."""
     import torch
     plan, P = dev["plan"], len(dev["points_um"])
+    main = torch.cuda.current_stream(plan.device)
+    stream = main if stream is None else stream
+    if stream is not main:
+        stream.wait_stream(main)
 
-    def host(t, key):
-        if out is not None and key in out:
-            out[key].copy_(t, non_blocking=True)
-            return out[key]
-        return t.cpu()
+    with torch.inference_mode(), torch.cuda.stream(stream):
+        def host(t, key):
+            dst = out[key] if out is not None and key in out else torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
+            dst.copy_(t, non_blocking=True)
+            if stream is not main:
+                t.record_stream(stream)
+            return dst
 
-    with torch.inference_mode():
-        masks_h = host(dev["masks"], "masks")
-        psf_abs = host(dev["psf_abs_sum"] / P, "psf")
-        psf_raw = host(dev["psf_sum"] / P, "psf_raw")
-        energies = host(dev["energies"], "energies")
-        psf_3d = host(dev["psf_3d"], "psf_3d") if return_psf_3d else None
-        prof = [host(p, f"profile{j}") for j, p in enumerate(dev["profiles"])]
-        wts = [host(w, f"weight{j}") for j, w in enumerate(dev["weights"])]
-        convs = [host(c, f"convmask{j}") for j, c in enumerate(dev["convmask"])]
         neg = -torch.clamp(dev["psf_3d"], max=0).sum(dtype=torch.float64) / torch.clamp(dev["psf_abs_sum"].sum(),
                                                                                           min=1e-30)
-        neg = float(neg)
-    torch.cuda.current_stream(plan.device).synchronize()
-    masks_h = masks_h.numpy()
+        h = {"masks": host(dev["masks"], "masks"), "psf": host(dev["psf_abs_sum"] / P, "psf"),
+             "psf_raw": host(dev["psf_sum"] / P, "psf_raw"), "energies": host(dev["energies"], "energies"),
+             "psf_3d": host(dev["psf_3d"], "psf_3d") if return_psf_3d else None,
+             "profiles": [host(p, f"profile{j}") for j, p in enumerate(dev["profiles"])],
+             "weights": [host(w, f"weight{j}") for j, w in enumerate(dev["weights"])],
+             "convmask": [host(c, f"convmask{j}") for j, c in enumerate(dev["convmask"])],
+             "neg": host(neg.reshape(1), "neg")}
+        done = torch.cuda.Event()
+        done.record(stream)
+    return {"dev": dev, "host": h, "event": done}
+
+
+def stage_result(config, pending):
+    """Host result dictionary (the keys of maomi.optics.propagate / assemble)
+    of a ``stage_copy_async`` once its copies have completed."""
+    pending["event"].synchronize()
+    dev, h = pending["dev"], pending["host"]
+    plan, P = dev["plan"], len(dev["points_um"])
+    masks_h = h["masks"].numpy()
     mask = masks_h[..., 0]
     mean = float(mask.mean())
     if not np.isfinite(mean) or mean <= 0:
         raise ValueError("Nonpositive or invalid mean excitation energy")
     result = {
-        "psf": psf_abs.numpy(), "psf_raw": psf_raw.numpy(),
-        "psf_3d": psf_3d.numpy() if psf_3d is not None else None,
-        "points_um": dev["points_um"], "energies": energies.numpy(),
+        "psf": h["psf"].numpy(), "psf_raw": h["psf_raw"].numpy(),
+        "psf_3d": h["psf_3d"].numpy() if h["psf_3d"] is not None else None,
+        "points_um": dev["points_um"], "energies": h["energies"].numpy(),
         "mask_raw": mask, "mask": mask / mean, "mask_mean": mean, "mask_mode": "matlab_v4",
         "tails_computed": dev["tails"], "unique_optical_paths": P,
-        "negative_resampling_mass_fraction": neg,
+        "negative_resampling_mass_fraction": float(h["neg"][0]),
     }
     if dev["tails"]:
         for j, name in enumerate(("psfT", "psfB")):
             z = plan.z_positions[0][plan.cut:] if j == 0 else plan.z_positions[2]
             tm = masks_h[..., j + 1]
             tm_mean = float(tm.mean())
-            prof_j, wts_j = prof[j].numpy(), wts[j].numpy()
+            prof_j, wts_j = h["profiles"][j].numpy(), h["weights"][j].numpy()
             result[name] = {
-                "convmask": convs[j].numpy(), "weight": float(wts_j.mean()),
+                "convmask": h["convmask"][j].numpy(), "weight": float(wts_j.mean()),
                 "psfZ": _psf_z(config, z, prof_j.sum(0)),
                 "mask_raw": tm, "mask": tm / tm_mean if tm_mean > 0 else tm, "mask_mean": tm_mean,
                 "weights_per_point": wts_j, "profiles_per_point": prof_j,
             }
     return result
+
+
+def stage_to_host(config, dev, *, return_psf_3d=True, out=None):
+    """Host result dictionary (the keys of maomi.optics.propagate / assemble)
+    from ``stage_device`` output.  ``out`` may hold pinned host buffers."""
+    return stage_result(config, stage_copy_async(dev, return_psf_3d=return_psf_3d, out=out))
+
+
+_PINNED_POOLS = {}
+
+
+def _pinned_set(dev, return_psf_3d):
+    """Pinned host buffers for every product of one stage (shapes of ``dev``)."""
+    import torch
+    items = {"masks": dev["masks"], "psf": dev["psf_abs_sum"], "psf_raw": dev["psf_sum"], "energies": dev["energies"]}
+    if return_psf_3d:
+        items["psf_3d"] = dev["psf_3d"]
+    for j in range(len(dev["profiles"])):
+        items[f"profile{j}"], items[f"weight{j}"] = dev["profiles"][j], dev["weights"][j]
+    for j in range(len(dev["convmask"])):
+        items[f"convmask{j}"] = dev["convmask"][j]
+    out = {k: torch.empty(t.shape, dtype=t.dtype, pin_memory=True) for k, t in items.items()}
+    out["neg"] = torch.empty(1, dtype=torch.float64, pin_memory=True)
+    return out
+
+
+def run_stages(config, blocks, points_um=None, *, device="cuda", depth=2, return_psf_3d=True, reuse=False,
+               **kwargs):
+    """Stage results of a sequence of tissue blocks (each three raw A/B/C
+    fields: NumPy arrays, pinned host tensors or device tensors), pipelined:
+    while block i's products are copied to the host on a copy stream, block
+    i+1 is uploaded and computed.  Yields the host dictionaries in order.
+
+    ``reuse=True`` copies into a pool of ``depth + 1`` pinned buffer sets kept
+    between calls (no page-locked allocation per block): a yielded result's
+    arrays stay valid until ``depth`` further results have been yielded."""
+    import collections
+    import torch
+    copy = torch.cuda.Stream(device=device)
+    pending = collections.deque()
+    count = 0
+    for raw in blocks:
+        fields = [a.to(device, non_blocking=True) if isinstance(a, torch.Tensor) else _lib.upload(a, device)
+                  for a in raw]
+        dev = stage_device(config, fields, points_um, device=device, **kwargs)
+        out = None
+        if reuse:
+            key = (str(device), tuple((k, tuple(v.shape)) for k, v in dev.items() if hasattr(v, "shape")),
+                   len(dev["profiles"]), bool(return_psf_3d), depth)
+            pool = _PINNED_POOLS.setdefault(key, [])
+            if len(pool) < depth + 1:
+                pool.append(_pinned_set(dev, return_psf_3d))
+            out = pool[count % (depth + 1)]
+        pending.append(stage_copy_async(dev, return_psf_3d=return_psf_3d, out=out, stream=copy))
+        count += 1
+        if len(pending) >= depth:
+            yield stage_result(config, pending.popleft())
+    while pending:
+        yield stage_result(config, pending.popleft())
 
 
 def run_stage(config, raw_fields, points_um=None, *, uin=None, device="cuda", tails=True, count_per_axis=65,

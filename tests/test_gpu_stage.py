@@ -222,3 +222,33 @@ def test_v4_lattice_parity_solve_matches_dense():
     m_tab = v4_evaluate_grid_device(p, c_lat, 512, 512, points_host=pts).cpu().numpy()
     np.testing.assert_array_equal(m_tab, m_lat)
     assert rel_l2(c_lat.cpu().numpy(), c_den.cpu().numpy()) < 1e-6
+
+
+@pytest.mark.gpu
+def test_pipelined_stages_match_single_runs(small):
+    """run_stages (upload of block i+1 and compute overlapping the copies of
+    block i) returns, block for block, what run_stage returns."""
+    import torch
+    from maomi_b200 import synthetic
+    from maomi_b200.fixed import run_stage, run_stages
+    from oracle import optics as O
+    d, cfg, raw = small
+    other = synthetic.raw_fields(cfg, O.field_shapes(cfg), sigma=2.0, rms=0.01, seed=99)
+    blocks = [raw, [torch.from_numpy(a).pin_memory() for a in other], raw]
+    got = list(run_stages(cfg, blocks, d["points"], device="cuda", precision="fp64"))
+    assert len(got) == 3
+    reused = [dict(r) for r in run_stages(cfg, blocks[:1], d["points"], device="cuda", precision="fp64",
+                                          reuse=True)]
+    np.testing.assert_array_equal(reused[0]["psf_3d"], got[0]["psf_3d"])
+    for res, src in zip(got, (raw, other, raw)):
+        ref = run_stage(cfg, src, d["points"], device="cuda", precision="fp64")
+        # psf_3d is deterministic; the site sums, energies and profiles are
+        # FP64 atomic sums whose order may differ between runs
+        np.testing.assert_array_equal(res["psf_3d"], ref["psf_3d"])
+        for key in ("psf", "psf_raw", "mask_raw", "energies"):
+            np.testing.assert_allclose(res[key], ref[key], rtol=1e-10, err_msg=key)
+        for t in ("psfT", "psfB"):
+            np.testing.assert_allclose(res[t]["convmask"], ref[t]["convmask"], rtol=1e-10)
+            np.testing.assert_allclose(res[t]["weight"], ref[t]["weight"], rtol=1e-10)
+        np.testing.assert_allclose(res["negative_resampling_mass_fraction"], ref["negative_resampling_mass_fraction"],
+                                   rtol=1e-10, atol=1e-300)
