@@ -57,7 +57,7 @@ def parse():
     ap.add_argument("--cpu-sites", type=int, default=8)
     ap.add_argument("--sites", type=int, default=SITES, help="profile a subset of the lattice (not a bench line)")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--precision", default="compensated", choices=["compensated", "mixed", "fp64", "fp32"])
+    ap.add_argument("--precision", default="compensated", choices=["compensated", "compensated-full", "mixed", "fp64", "fp32"])
     ap.add_argument("--workload", default="stage", choices=["stage", "surrogate", "uneven", "local"],
                     help="stage: the headline optical stage; surrogate: the learned PSF path with its plain gate; "
                          "uneven: 6,000 mixed-size items in one graph; local: the local-PSF render")

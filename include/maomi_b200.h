@@ -206,9 +206,10 @@ typedef struct {
   int nsites;
   int precision;           /* arithmetic of the radix-2 line transforms: FP32,
                               FP64 (butterflies, twiddles and filter in FP64),
-                              MIXED (forward FP32, inverse FP64) or COMPENSATED
-                              (FP32 butterflies, every DFT rotation and twiddle
-                              constant carried as a hi + lo pair of floats); the
+                              MIXED (forward FP32, inverse FP64), COMPENSATED
+                              (FP32 butterflies, every DFT rotation constant
+                              carried as a hi + lo pair of floats) or
+                              COMPENSATED_FULL (the twiddle tables too); the
                               field is stored complex64 in every mode             */
   int reserve_sms;         /* persistent schedule: CTAs that start on SM ids below
                               this count leave at once, so work queued on other
@@ -216,7 +217,13 @@ typedef struct {
                               while the sites propagate; 0 = use every SM         */
 } mm_stage_plan;
 
-enum { MM_PRECISION_FP32 = 0, MM_PRECISION_FP64 = 1, MM_PRECISION_MIXED = 2, MM_PRECISION_COMPENSATED = 3 };
+enum {
+  MM_PRECISION_FP32 = 0,
+  MM_PRECISION_FP64 = 1,
+  MM_PRECISION_MIXED = 2,
+  MM_PRECISION_COMPENSATED = 3,
+  MM_PRECISION_COMPENSATED_FULL = 4
+};
 
 enum { MM_SCHEDULE_PERSISTENT = 0, MM_SCHEDULE_BATCHED = 1 };
 

@@ -14,9 +14,10 @@ LIB_PATH = Path(__file__).resolve().parent / "libmaomi_b200.so"
 
 MM_OK, MM_ERR_ARGUMENT, MM_ERR_CUDA, MM_ERR_TIMEOUT, MM_ERR_NONFINITE, MM_ERR_UNSUPPORTED = 0, -1, -2, -3, -4, -5
 MM_SCHEDULE_PERSISTENT, MM_SCHEDULE_BATCHED = 0, 1
-MM_PRECISION_FP32, MM_PRECISION_FP64, MM_PRECISION_MIXED, MM_PRECISION_COMPENSATED = 0, 1, 2, 3
+MM_PRECISION_FP32, MM_PRECISION_FP64, MM_PRECISION_MIXED = 0, 1, 2
+MM_PRECISION_COMPENSATED, MM_PRECISION_COMPENSATED_FULL = 3, 4
 PRECISIONS = {"fp32": MM_PRECISION_FP32, "fp64": MM_PRECISION_FP64, "mixed": MM_PRECISION_MIXED,
-              "compensated": MM_PRECISION_COMPENSATED}
+              "compensated": MM_PRECISION_COMPENSATED, "compensated-full": MM_PRECISION_COMPENSATED_FULL}
 
 c_int_p = POINTER(c_int)
 c_float_p = POINTER(c_float)

@@ -101,7 +101,8 @@ class OpticalPlan:
         if precision not in _lib.PRECISIONS:
             raise ValueError("precision must be one of " + ", ".join(_lib.PRECISIONS))
         #: arithmetic of the radix-2 line transforms: "compensated" (FP32
-        #: butterflies, rotation and twiddle constants as hi + lo float pairs),
+        #: butterflies, DFT rotation constants as hi + lo float pairs),
+        #: "compensated-full" (the twiddle tables too),
         #: "fp64" (FP64 butterflies, twiddles and filter), "mixed" (forward
         #: FP32, inverse FP64) or "fp32"; fields are stored complex64 in every mode
         self.precision = precision

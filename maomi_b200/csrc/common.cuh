@@ -53,20 +53,31 @@ __host__ __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
 __host__ __device__ __forceinline__ double2 cmul(double2 a, float2 b) { return cmul(a, make_double2(b.x, b.y)); }
 __host__ __device__ __forceinline__ double cnorm2(double2 a) { return a.x * a.x + a.y * a.y; }
 
-// FP32 complex arithmetic whose multiplications by constants (the DFT
-// rotations and twiddles) take each constant as an unevaluated pair
-// hi + lo of floats.  The rounding of a constant is the same in every
-// transform, so its error adds up coherently over hundreds of line
-// transforms; carrying the constant to ~2^-48 leaves only the data-dependent
-// (incoherent) roundings of FP32 butterflies.
-struct __align__(8) cfx {
+// FP32 complex arithmetic whose multiplications by the DFT rotation
+// constants take each constant as an unevaluated pair hi + lo of floats; with
+// TW the twiddle tables are carried the same way (entries {hi, lo}).  The
+// rounding of a constant is the same in every transform, so its error adds up
+// coherently over hundreds of line transforms; carrying the constant to
+// ~2^-48 leaves only the data-dependent (incoherent) roundings of FP32
+// butterflies.  The rotations dominate that coherent error, the twiddle
+// tables add a smaller share.
+template <bool TW>
+struct __align__(8) cfx_t {
   float x, y;
 };
-__host__ __device__ __forceinline__ cfx cadd(cfx a, cfx b) { return cfx{a.x + b.x, a.y + b.y}; }
-__host__ __device__ __forceinline__ cfx csub(cfx a, cfx b) { return cfx{a.x - b.x, a.y - b.y}; }
-// a * b for a data value b (the filter): plain FP32.
-__host__ __device__ __forceinline__ cfx cmul(cfx a, float2 b) {
-  return cfx{a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x};
+using cfx = cfx_t<true>;   // rotations and twiddle tables compensated
+using cfr = cfx_t<false>;  // rotations compensated, FP32 twiddle tables
+template <class C> struct IsCompensated { static constexpr bool value = false; };
+template <bool TW> struct IsCompensated<cfx_t<TW>> { static constexpr bool value = true; };
+
+template <bool TW>
+__host__ __device__ __forceinline__ cfx_t<TW> cadd(cfx_t<TW> a, cfx_t<TW> b) { return {a.x + b.x, a.y + b.y}; }
+template <bool TW>
+__host__ __device__ __forceinline__ cfx_t<TW> csub(cfx_t<TW> a, cfx_t<TW> b) { return {a.x - b.x, a.y - b.y}; }
+// a * b for a data value or a plain FP32 twiddle b: ordinary FP32 product.
+template <bool TW>
+__host__ __device__ __forceinline__ cfx_t<TW> cmul(cfx_t<TW> a, float2 b) {
+  return {a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x};
 }
 // a * w for a constant w = (hi.x + lo.x) + i (hi.y + lo.y), packed {hi.x, hi.y, lo.x, lo.y}.
 __device__ __forceinline__ cfx cmul(cfx a, float4 w) {
@@ -88,12 +99,13 @@ template <class C> __device__ __forceinline__ C make_c(double re, double im);
 template <> __device__ __forceinline__ float2 make_c<float2>(double re, double im) { return make_float2(float(re), float(im)); }
 template <> __device__ __forceinline__ double2 make_c<double2>(double re, double im) { return make_double2(re, im); }
 template <> __device__ __forceinline__ cfx from_f2<cfx>(float2 a) { return cfx{a.x, a.y}; }
-__device__ __forceinline__ float2 to_f2(cfx a) { return make_float2(a.x, a.y); }
-template <class C> __device__ __forceinline__ C promote(cfx a);
-template <> __device__ __forceinline__ cfx promote<cfx>(cfx a) { return a; }
+template <> __device__ __forceinline__ cfr from_f2<cfr>(float2 a) { return cfr{a.x, a.y}; }
+template <bool TW> __device__ __forceinline__ float2 to_f2(cfx_t<TW> a) { return make_float2(a.x, a.y); }
+template <class C, bool TW> __device__ __forceinline__ C promote(cfx_t<TW> a) { return a; }
 // Twiddle-table entries of a register type: cfx keeps {hi, lo} pairs.
 template <class C> struct TwiddleOf { using T = C; };
 template <> struct TwiddleOf<cfx> { using T = float4; };
+template <> struct TwiddleOf<cfr> { using T = float2; };
 template <class T> __device__ __forceinline__ T make_tw(double re, double im) { return make_c<T>(re, im); }
 template <> __device__ __forceinline__ float4 make_tw<float4>(double re, double im) {
   const float hx = float(re), hy = float(im);
@@ -105,9 +117,9 @@ template <int SIGN>
 __device__ __forceinline__ float2 quarter(float2 a) {
   return SIGN < 0 ? make_float2(a.y, -a.x) : make_float2(-a.y, a.x);
 }
-template <int SIGN>
-__device__ __forceinline__ cfx quarter(cfx a) {
-  return SIGN < 0 ? cfx{a.y, -a.x} : cfx{-a.y, a.x};
+template <int SIGN, bool TW>
+__device__ __forceinline__ cfx_t<TW> quarter(cfx_t<TW> a) {
+  return SIGN < 0 ? cfx_t<TW>{a.y, -a.x} : cfx_t<TW>{-a.y, a.x};
 }
 template <int SIGN>
 __device__ __forceinline__ double2 quarter(double2 a) {

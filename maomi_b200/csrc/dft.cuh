@@ -39,7 +39,7 @@ __device__ constexpr double kSin16[17] = {
 template <class C> struct Real;
 template <> struct Real<float2> { using T = float; };
 template <> struct Real<double2> { using T = double; };
-template <> struct Real<cfx> { using T = float; };
+template <bool TW> struct Real<cfx_t<TW>> { using T = float; };
 
 // a * W_32^k with W = exp(SIGN * 2*pi*i/32), k = 0..15 (angle pi*k/16).
 template <int SIGN, int K, class C>
@@ -49,7 +49,7 @@ __device__ __forceinline__ C rot32(C a) {
     return a;
   } else if constexpr (K == 8) {
     return quarter<SIGN>(a);
-  } else if constexpr (std::is_same_v<C, cfx>) {
+  } else if constexpr (IsCompensated<C>::value) {
     // constants as hi + lo float pairs (see cfx)
     constexpr double c = kCos16[K], s = SIGN * kSin16[K];
     constexpr float ch = float(c), sh = float(s);
@@ -59,10 +59,10 @@ __device__ __forceinline__ C rot32(C a) {
       constexpr float g = c > 0 ? ch : -ch, gl = c > 0 ? cl : -cl;  // +sqrt(1/2) as hi + lo
       constexpr float ex = c > 0 ? 1.f : -1.f, ey = s > 0 ? 1.f : -1.f;
       const float u = ex * a.x - ey * a.y, w = ey * a.x + ex * a.y;
-      return cfx{fmaf(u, g, u * gl), fmaf(w, g, w * gl)};
+      return C{fmaf(u, g, u * gl), fmaf(w, g, w * gl)};
     } else {
       const float rx = fmaf(a.x, cl, -a.y * sl), ry = fmaf(a.x, sl, a.y * cl);
-      return cfx{fmaf(a.x, ch, fmaf(-a.y, sh, rx)), fmaf(a.x, sh, fmaf(a.y, ch, ry))};
+      return C{fmaf(a.x, ch, fmaf(-a.y, sh, rx)), fmaf(a.x, sh, fmaf(a.y, ch, ry))};
     }
   } else {
     const T c = T(kCos16[K]), s = T(SIGN * kSin16[K]);
@@ -201,8 +201,9 @@ __device__ __forceinline__ void dft(C* v) {
 // exchange suffices.
 //
 // CF / CI are the register arithmetic types of the forward and the inverse
-// half: float2 (FP32), cfx (FP32 butterflies, constants as hi + lo pairs) or
-// double2 (FP64 butterflies, twiddles and filter).
+// half: float2 (FP32), cfr / cfx (FP32 butterflies, rotation constants as
+// hi + lo pairs; cfx also the twiddle tables) or double2 (FP64 butterflies,
+// twiddles and filter).
 // The line enters and leaves as complex64 and the exchanges are complex64.
 // The inverse half carries most of the rounding that reaches the saved
 // intensities, so <float2, double2> ("mixed") recovers most of the FP64
@@ -229,9 +230,9 @@ struct FftLine {
   static constexpr bool kFft = true;
   static constexpr size_t kTwiddleBytes = (size_t)N * (sizeof(TF) + sizeof(TI));
   // CTAs of 128 threads resident per SM the kernels are compiled for: the
-  // FP32 forms fit in 96 registers (5 CTAs); FP64 halves need the 4-CTA budget.
+  // FP32 forms fit in 80 registers (6 CTAs); FP64 halves need the 4-CTA budget.
   static constexpr int kMinBlocks =
-      R1 > 16 ? 2 : ((std::is_same_v<CF, double2> || std::is_same_v<CI, double2>) ? 4 : 5);
+      R1 > 16 ? 2 : ((std::is_same_v<CF, double2> || std::is_same_v<CI, double2>) ? 4 : 6);
   static_assert(R1 % R2 == 0, "R2 must divide R1");
 
   // twf[k1*R2 + t] = W_N^(t*k1) (CF);  twi[n*R1 + k1] = W_N^(-n*k1) (CI).

@@ -257,7 +257,8 @@ extern "C" int mm_propagate_items(const mm_item_class* c, void* workspace, size_
   MM_CHECK_ARG(c->nitems >= 0 && c->slots >= 1 && c->waves >= 0, "bad item counts");
   MM_CHECK_ARG(c->shape == 0 || c->shape == 1, "unknown shape %d", c->shape);
   MM_CHECK_ARG(c->precision == MM_PRECISION_FP32 || c->precision == MM_PRECISION_FP64 ||
-                   c->precision == MM_PRECISION_MIXED || c->precision == MM_PRECISION_COMPENSATED,
+                   c->precision == MM_PRECISION_MIXED || c->precision == MM_PRECISION_COMPENSATED ||
+                   c->precision == MM_PRECISION_COMPENSATED_FULL,
                "unknown precision %d", c->precision);
   if (c->nitems == 0) return MM_OK;
   MM_CHECK_ARG(c->steps && c->phase_offset && c->phase && c->field_in && c->field_out && c->kernel &&
@@ -288,7 +289,8 @@ extern "C" int mm_propagate_items(const mm_item_class* c, void* workspace, size_
   int rc;
   if (c->precision == MM_PRECISION_FP64) rc = ilaunch_any<double2, double2>(p, c->shape, s);
   else if (c->precision == MM_PRECISION_MIXED) rc = ilaunch_any<float2, double2>(p, c->shape, s);
-  else if (c->precision == MM_PRECISION_COMPENSATED) rc = ilaunch_any<cfx, cfx>(p, c->shape, s);
+  else if (c->precision == MM_PRECISION_COMPENSATED) rc = ilaunch_any<cfr, cfr>(p, c->shape, s);
+  else if (c->precision == MM_PRECISION_COMPENSATED_FULL) rc = ilaunch_any<cfx, cfx>(p, c->shape, s);
   else rc = ilaunch_any<float2, float2>(p, c->shape, s);
   if (rc != MM_OK || !check) return rc;
   MM_CHECK_CUDA(cudaStreamSynchronize(s), "item propagation");

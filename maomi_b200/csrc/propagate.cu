@@ -154,32 +154,10 @@ __device__ __forceinline__ int2 site_offset(const Params& p, const Item& it) {
   return make_int2(xo, yo);
 }
 
-// Start the asynchronous copy of this thread's screen samples into shared
-// memory (slot j*blockDim + tid); they are consumed after the first half step.
-template <class L, int LINES>
-__device__ void prefetch_screen(const Params& p, const Item& it, float2* scr_s) {
-  const StageP& st = p.st[it.stage];
-  if (it.k >= st.steps) return;
-  const Lane<L, LINES> ln(p, it);
-  const int N = st.size;
-  const int2 o = site_offset(p, it);
-  // element j of this thread sits at base + j*step in the (vol_h, vol_w) plane
-  const int row0 = ln.axis == 0 ? ln.line : ln.t, col0 = ln.axis == 0 ? ln.t : ln.line;
-  const float2* scr = st.screens + (size_t)it.k * st.vol_h * st.vol_w + (size_t)(o.x + row0) * st.vol_w + (o.y + col0);
-  const size_t step = ln.axis == 0 ? size_t(L::R2) : size_t(L::R2) * st.vol_w;
-#pragma unroll
-  for (int j = 0; j < L::R1; ++j) {
-    const int e = ln.t + L::R2 * j;
-    if (!(L::kFft || (ln.line < N && e < N))) continue;
-    cp_async8(scr_s + j * blockDim.x + threadIdx.x, scr + j * step);
-  }
-  cp_async_commit();
-}
-
 // One (site, segment, line block) work item.
 template <class L, int LINES>
 __device__ void process(const Params& p, const Item& it, float2* xa, float2* xb, const typename L::TF* twf,
-                        const typename L::TI* twi, float* red, const float2* scr_s) {
+                        const typename L::TI* twi, float* red) {
   constexpr int R1 = L::R1, R2 = L::R2;
   const StageP& st = p.st[it.stage];
   const int N = st.size;
@@ -236,14 +214,21 @@ __device__ void process(const Params& p, const Item& it, float2* xa, float2* xb,
     L::template propagate<true>(v, t, st.kern + (size_t)(it.k - 1) * N, N, xa_l, xb_l, twf, twi, warp_local);
   // ------------------------------------------------------- screen of step k
   if (it.k < st.steps) {
+    // the screen samples at the site's window offset, read straight from the
+    // (Z, H, W) volume: issued together, consumed after all have arrived
     const float eline = live ? __ldg(st.edge + line) : 0.f;
-    cp_async_wait_all();
+    const int2 so = site_offset(p, it);
+    const float2* scr = st.screens + (size_t)it.k * st.vol_h * st.vol_w + (size_t)(so.x + row0) * st.vol_w + (so.y + col0);
+    const size_t sstep = axis == 0 ? size_t(R2) : size_t(R2) * st.vol_w;
+    float2 sv[R1];
+#pragma unroll
+    for (int j = 0; j < R1; ++j) sv[j] = in_line(t + R2 * j) ? __ldg(scr + j * sstep) : make_float2(0.f, 0.f);
 #pragma unroll
     for (int j = 0; j < R1; ++j) {
       const int e = t + R2 * j;
       if (!in_line(e)) continue;
       const float w = axis == 0 ? eline * __ldg(st.edge + e) : __ldg(st.edge + e) * eline;
-      float2 s = scr_s[j * blockDim.x + threadIdx.x];
+      float2 s = sv[j];
       s = make_float2(s.x * w, s.y * w);
       v[j] = cmul(v[j], s);
     }
@@ -305,9 +290,7 @@ __device__ void process(const Params& p, const Item& it, float2* xa, float2* xb,
 template <class L, int LINES>
 struct Smem {
   static constexpr size_t xbuf = (size_t)LINES * L::XBUF;     // float2 per exchange buffer (even count)
-  static constexpr size_t screen = (size_t)LINES * L::R2 * L::R1;  // float2: one screen tile
-  static constexpr size_t bytes =
-      (xbuf + xbuf % 2) * sizeof(float2) + L::kTwiddleBytes + screen * sizeof(float2) + 32 * sizeof(float);
+  static constexpr size_t bytes = (xbuf + xbuf % 2) * sizeof(float2) + L::kTwiddleBytes + 32 * sizeof(float);
 };
 
 template <class L, int LINES>
@@ -317,8 +300,7 @@ __global__ void __launch_bounds__(LINES * L::R2, L::kMinBlocks * 128 / (LINES * 
   float2* xb = xa;
   auto* twf = reinterpret_cast<typename L::TF*>(xa + Smem<L, LINES>::xbuf + Smem<L, LINES>::xbuf % 2);
   auto* twi = reinterpret_cast<typename L::TI*>(reinterpret_cast<char*>(twf) + (L::kFft ? L::N * sizeof(typename L::TF) : 0));
-  float2* scr_s = reinterpret_cast<float2*>(reinterpret_cast<char*>(twi) + (L::kFft ? L::N * sizeof(typename L::TI) : 0));
-  float* red = reinterpret_cast<float*>(scr_s + Smem<L, LINES>::screen);
+  float* red = reinterpret_cast<float*>(reinterpret_cast<char*>(twi) + (L::kFft ? L::N * sizeof(typename L::TI) : 0));
   __shared__ long long s_item;
   __shared__ int s_abort;
   if (p.reserve_sms > 0) {
@@ -339,7 +321,6 @@ __global__ void __launch_bounds__(LINES * L::R2, L::kMinBlocks * 128 / (LINES * 
     Item it;
     const bool live = decode(p, item, it);
     if (live) {
-      prefetch_screen<L, LINES>(p, it, scr_s);  // inputs only: safe before the dependency wait
       if (threadIdx.x == 0) {
         const StageP& st = p.st[it.stage];
         const unsigned need = unsigned(it.wave * p.blocks_per_site + st.cum0 + (long long)it.k * st.nblocks);
@@ -359,7 +340,7 @@ __global__ void __launch_bounds__(LINES * L::R2, L::kMinBlocks * 128 / (LINES * 
       }
       __syncthreads();
       if (s_abort) break;
-      process<L, LINES>(p, it, xa, xb, twf, twi, red, scr_s);
+      process<L, LINES>(p, it, xa, xb, twf, twi, red);
       __syncthreads();
       if (threadIdx.x == 0) {
         // release: the CTA's field stores (ordered by the barrier) become
@@ -381,8 +362,7 @@ __global__ void __launch_bounds__(LINES * L::R2, L::kMinBlocks * 128 / (LINES * 
   float2* xb = xa;
   auto* twf = reinterpret_cast<typename L::TF*>(xa + Smem<L, LINES>::xbuf + Smem<L, LINES>::xbuf % 2);
   auto* twi = reinterpret_cast<typename L::TI*>(reinterpret_cast<char*>(twf) + (L::kFft ? L::N * sizeof(typename L::TF) : 0));
-  float2* scr_s = reinterpret_cast<float2*>(reinterpret_cast<char*>(twi) + (L::kFft ? L::N * sizeof(typename L::TI) : 0));
-  float* red = reinterpret_cast<float*>(scr_s + Smem<L, LINES>::screen);
+  float* red = reinterpret_cast<float*>(reinterpret_cast<char*>(twi) + (L::kFft ? L::N * sizeof(typename L::TI) : 0));
   fill_twiddles<L>(twf, twi);
   __syncthreads();
   const StageP& st = p.st[p.b_stage];
@@ -394,8 +374,7 @@ __global__ void __launch_bounds__(LINES * L::R2, L::kMinBlocks * 128 / (LINES * 
   it.site = p.b_site0 + it.slot;
   it.wave = 0;
   if (it.site >= p.nsites) return;
-  prefetch_screen<L, LINES>(p, it, scr_s);
-  process<L, LINES>(p, it, xa, xb, twf, twi, red, scr_s);
+  process<L, LINES>(p, it, xa, xb, twf, twi, red);
 }
 
 // ------------------------------------------------------------------- host --
@@ -483,7 +462,8 @@ int launch_batched_any(Params& p, int stage, int k, int site0, int batch, cudaSt
     case 512:
       if (p.precision == MM_PRECISION_FP64) return launch_batched_fft<double2, double2>(p, stage, k, site0, batch, s);
       if (p.precision == MM_PRECISION_MIXED) return launch_batched_fft<float2, double2>(p, stage, k, site0, batch, s);
-      if (p.precision == MM_PRECISION_COMPENSATED) return launch_batched_fft<cfx, cfx>(p, stage, k, site0, batch, s);
+      if (p.precision == MM_PRECISION_COMPENSATED) return launch_batched_fft<cfr, cfr>(p, stage, k, site0, batch, s);
+      if (p.precision == MM_PRECISION_COMPENSATED_FULL) return launch_batched_fft<cfx, cfx>(p, stage, k, site0, batch, s);
       return launch_batched_fft<float2, float2>(p, stage, k, site0, batch, s);
     default:
       if (n <= 128) return launch_batched<DenseLine<8>, kLinesDense>(p, stage, k, site0, batch, s);
@@ -528,7 +508,8 @@ int launch_persistent_any(Params& p, cudaStream_t s) {
   }
   if (p.precision == MM_PRECISION_FP64) return launch_persistent_fft<double2, double2>(p, s);
   if (p.precision == MM_PRECISION_MIXED) return launch_persistent_fft<float2, double2>(p, s);
-  if (p.precision == MM_PRECISION_COMPENSATED) return launch_persistent_fft<cfx, cfx>(p, s);
+  if (p.precision == MM_PRECISION_COMPENSATED) return launch_persistent_fft<cfr, cfr>(p, s);
+  if (p.precision == MM_PRECISION_COMPENSATED_FULL) return launch_persistent_fft<cfx, cfx>(p, s);
   return launch_persistent_fft<float2, float2>(p, s);
 }
 
@@ -598,7 +579,8 @@ int build_params(const mm_stage_plan* plan, int slots, Params& p) {
   p.nsites = plan->nsites;
   p.slots = slots;
   MM_CHECK_ARG(plan->precision == MM_PRECISION_FP32 || plan->precision == MM_PRECISION_FP64 ||
-                   plan->precision == MM_PRECISION_MIXED || plan->precision == MM_PRECISION_COMPENSATED,
+                   plan->precision == MM_PRECISION_MIXED || plan->precision == MM_PRECISION_COMPENSATED ||
+                   plan->precision == MM_PRECISION_COMPENSATED_FULL,
                "unknown precision %d", plan->precision);
   p.precision = plan->precision;
   MM_CHECK_ARG(plan->reserve_sms >= 0 && plan->reserve_sms <= 64, "reserve_sms %d outside 0..64", plan->reserve_sms);
