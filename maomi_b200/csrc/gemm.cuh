@@ -24,7 +24,7 @@
 namespace mm {
 namespace gemm {
 
-constexpr int kStages = 4;
+constexpr int kStages = 4;  // default ring depth (long-K spectral GEMMs)
 constexpr int kBM = 128;               // rows per tile
 constexpr int kBK = 64;                // K elements per stage (one 128-byte swizzle row)
 constexpr int kATile = kBM * kBK * 2;  // bytes
@@ -44,11 +44,11 @@ struct Tiles {
   int* err;
 };
 
-template <int NT, int NB>
+template <int NT, int NB, int ST = kStages>
 struct Smem {
   static constexpr int kBTile = NT * kBK * 2;
   static constexpr int kStage = kATile + kBTile;
-  static constexpr size_t bytes = 1024 + (size_t)kStages * kStage + 256;
+  static constexpr size_t bytes = 1024 + (size_t)ST * kStage + 256;
 };
 
 template <int NT>
@@ -56,14 +56,15 @@ __host__ __device__ constexpr uint32_t tmem_cols() {
   return NT <= 32 ? 32u : (NT <= 64 ? 64u : (NT <= 128 ? 128u : 256u));
 }
 
-template <int NT, int NB, class Epi>
+template <int NT, int NB, class Epi, int ST = kStages>
 __global__ void __launch_bounds__(128, 1)
     gemm_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
                 const __grid_constant__ CUtensorMap mapA2, const __grid_constant__ CUtensorMap mapB2, Tiles t,
                 Epi epi) {
   static_assert(NT % 16 == 0 && NT >= 16 && NT <= 256, "wide N");
   static_assert(NB % 16 == 0 && NB >= 16 && NB <= 64, "sub-block N");
-  using S = Smem<NT, NB>;
+  using S = Smem<NT, NB, ST>;
+  constexpr int kStages = ST;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint64_t* full = reinterpret_cast<uint64_t*>(base + kStages * S::kStage);

@@ -15,11 +15,11 @@ namespace mm {
 namespace {
 
 // ------------------------------------------------------------ launching --
-template <int NT, int NB, class Epi>
+template <int NT, int NB, class Epi, int ST = gemm::kStages>
 int launch_gemm(const CUtensorMap& a, const CUtensorMap& b, const CUtensorMap& a2, const CUtensorMap& b2,
                 const gemm::Tiles& t, dim3 grid, const Epi& epi, cudaStream_t s) {
-  auto kernel = gemm::gemm_kernel<NT, NB, Epi>;
-  const size_t smem = gemm::Smem<NT, NB>::bytes;
+  auto kernel = gemm::gemm_kernel<NT, NB, Epi, ST>;
+  const size_t smem = gemm::Smem<NT, NB, ST>::bytes;
   MM_CHECK_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
                 "cudaFuncSetAttribute(gemm)");
   int per_sm = 0;
@@ -127,7 +127,7 @@ struct EpiSpectral {
   }
 };
 
-// Store one pixel's 32 channels of site s in both layouts (BF16).
+// Store one pixel's 32 channels of site s in both layouts (BF16); hc may be NULL.
 __device__ __forceinline__ void store_both(__nv_bfloat16* hp, __nv_bfloat16* hc, int s, int pix, const float (&h)[32]) {
   uint4* dp = reinterpret_cast<uint4*>(hp + ((size_t)s * kPix + pix) * kWidth);
 #pragma unroll
@@ -141,6 +141,7 @@ __device__ __forceinline__ void store_both(__nv_bfloat16* hp, __nv_bfloat16* hc,
     u.w = *reinterpret_cast<uint32_t*>(&d);
     dp[k] = u;
   }
+  if (!hc) return;
   __nv_bfloat16* dc = hc + (size_t)s * kWidth * kPix + pix;
 #pragma unroll
   for (int o = 0; o < kWidth; ++o) dc[(size_t)o * kPix] = __float2bfloat16_rn(h[o]);
@@ -150,7 +151,7 @@ __device__ __forceinline__ void store_both(__nv_bfloat16* hp, __nv_bfloat16* hc,
 struct EpiLayer {
   const float* bias;
   float* z;  // (S, 4096, 32) or NULL
-  __nv_bfloat16 *hp, *hc;
+  __nv_bfloat16 *hp, *hc;  // hc NULL: pixel-major copy only
   int sites, act;
   __device__ void store(int bx, int by, int row, int c, const float (&v)[32]) const {
     const int pix = bx * gemm::kBM + row, s = by * kGroup + c / kWidth;
@@ -557,7 +558,9 @@ int fused(const void* A, const void* coef_c, const void* act_p, const void* W, i
   t.ncols = 256;
   t.err = err;
   const dim3 grid(kPix / gemm::kBM, (S + kGroup - 1) / kGroup);
-  return launch_gemm<256, 32>(m.a, m.b, m.a2, m.b2, t, grid, epi, s);
+  // short K (9 blocks + 8 pointwise blocks) and a heavy epilogue: a 2-stage
+  // ring fits two CTAs per SM, so one CTA's epilogue overlaps the other's loads
+  return launch_gemm<256, 32, Epi, 2>(m.a, m.b, m.a2, m.b2, t, grid, epi, s);
 }
 
 // Pointwise-only GEMM: acc[pix, (site, n)] = act_p (S*4096 x kin) * W (NB x kin)^T per site.
@@ -573,7 +576,7 @@ int pointwise(const void* act_p, int kin, const void* W, int S, int* err, const 
   t.ncols = kGroup * NB;
   t.err = err;
   const dim3 grid(kPix / gemm::kBM, (S + kGroup - 1) / kGroup);
-  return launch_gemm<kGroup * NB, NB>(m.a2, m.b2, m.a2, m.b2, t, grid, epi, s);
+  return launch_gemm<kGroup * NB, NB, Epi, 2>(m.a2, m.b2, m.a2, m.b2, t, grid, epi, s);
 }
 
 // Weight gradient dW[a][b] += sum_(site,pix) g[(site, a), pix] * act[(site, b), pix]
@@ -717,7 +720,11 @@ extern "C" int mm_surrogate_forward(const mm_surrogate_desc* d, int check, void*
     mix_forward_kernel<<<dim3(kNModes, (S + 63) / 64), 256, 0, s>>>(d->v[l], d->params + off_rr(l),
                                                                        d->params + off_ri(l), bf(d->voc), S);
     MM_CHECK_LAUNCH("surrogate spectral mixing");
-    const EpiLayer epi{d->params + off_b(l), d->z[l], bf(d->hp[l + 1]), bf(d->hc[l + 1]), S, l < kLayers - 1};
+    // without pre-activation buffers (inference) the last layer's
+    // channel-major copy, only read by the backward pass, is skipped too
+    const bool train = d->z[0] != nullptr;
+    const EpiLayer epi{d->params + off_b(l), train ? d->z[l] : nullptr, bf(d->hp[l + 1]),
+                       (train || l < kLayers - 1) ? bf(d->hc[l + 1]) : nullptr, S, l < kLayers - 1};
     if (int rc = fused(d->G, d->voc, d->hp[l], d->wb[l], S, d->err, epi, s)) return rc;
   }
   if (int rc = pointwise<16>(d->hp[kLayers], kWidth, d->wpb, S, d->err,

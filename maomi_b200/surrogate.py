@@ -165,7 +165,7 @@ class PSFSurrogate:
         self._bufs[S] = b
         return b
 
-    def _desc(self, S, xp, xc):
+    def _desc(self, S, xp, xc, train=True):
         b = self._buffers(S)
         d = SurrogateDesc()
         d.sites = S
@@ -173,7 +173,7 @@ class PSFSurrogate:
         d.params, d.grads = self.params.data_ptr(), self.grads.data_ptr()
         for l in range(LAYERS):
             d.wb[l], d.wtb[l], d.v[l] = self.wb[l].data_ptr(), self.wtb[l].data_ptr(), b["v"][l].data_ptr()
-            d.z[l] = b["z"][l].data_ptr() if l < LAYERS - 1 else None
+            d.z[l] = b["z"][l].data_ptr() if (train and l < LAYERS - 1) else None
         d.wlb, d.wpb, d.wptb = self.wlb.data_ptr(), self.wpb.data_ptr(), self.wptb.data_ptr()
         d.base = self.base.data_ptr()
         d.xp, d.xc = xp.data_ptr(), xc.data_ptr()
@@ -200,10 +200,11 @@ class PSFSurrogate:
         return S
 
     # ------------------------------------------------------------ execution
-    def forward(self, xp, xc, *, check=False):
-        """Prediction (S, 4096, 16) FP32 for S sites of pixel- and channel-major inputs."""
+    def forward(self, xp, xc, *, check=False, train=True):
+        """Prediction (S, 4096, 16) FP32 for S sites of pixel- and channel-major
+        inputs.  ``train=False`` skips the stores only the backward pass reads."""
         S = self._check_inputs(xp, xc)
-        d, b = self._desc(S, xp, xc)
+        d, b = self._desc(S, xp, xc, train)
         self._d = d
         _lib.check(_lib.load().mm_surrogate_forward(d, int(check), _lib.stream_of(self.device)),
                    "surrogate forward")
@@ -263,7 +264,7 @@ class PSFSurrogate:
         xp3, xc3 = xp.view(S, NPIX, WIDTH), xc.view(S, WIDTH, NPIX)
         for s0 in range(0, S, batch):
             s1 = min(S, s0 + batch)
-            y = self.forward(xp3[s0:s1].reshape(-1, WIDTH), xc3[s0:s1].reshape(-1, NPIX))
+            y = self.forward(xp3[s0:s1].reshape(-1, WIDTH), xc3[s0:s1].reshape(-1, NPIX), train=False)
             _lib.check(_lib.load().mm_surrogate_planes(y.data_ptr(), out[s0:s1].data_ptr(), s1 - s0,
                                                         _lib.stream_of(self.device)), "surrogate planes")
         return out
