@@ -253,3 +253,18 @@ def test_pipelined_stages_match_single_runs(small):
             np.testing.assert_allclose(res[t]["weight"], ref[t]["weight"], rtol=1e-10)
         np.testing.assert_allclose(res["negative_resampling_mass_fraction"], ref["negative_resampling_mass_fraction"],
                                    rtol=1e-10, atol=1e-300)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("nx,ny", [(4, 5), (7, 6), (2, 3)])
+def test_v4_parity_blocks_small_lattices(nx, ny):
+    """Even and odd lattice sizes (with and without a centre row/column),
+    shuffled point order: the parity-block solve equals the dense LU."""
+    from maomi_b200.numerics import lattice_index, v4_factor_device, v4_solve_device
+    rng = np.random.default_rng(nx * 10 + ny)
+    pts = np.array([(8.0 * i, 8.0 * j + 4.0) for i in range(nx) for j in range(ny)])[rng.permutation(nx * ny)]
+    assert lattice_index(pts) is not None
+    vals = rng.normal(size=(len(pts), 3))
+    _, a = v4_solve_device(v4_factor_device(pts), vals)
+    _, b = v4_solve_device(v4_factor_device(pts, structured=False), vals)
+    assert rel_l2(a.cpu().numpy(), b.cpu().numpy()) < 1e-10
