@@ -268,3 +268,20 @@ def test_v4_parity_blocks_small_lattices(nx, ny):
     _, a = v4_solve_device(v4_factor_device(pts), vals)
     _, b = v4_solve_device(v4_factor_device(pts, structured=False), vals)
     assert rel_l2(a.cpu().numpy(), b.cpu().numpy()) < 1e-10
+
+
+def test_single_site_stage_matches_oracle_fp64(small):
+    """One site: the v4 masks degenerate to the site's constant values (the
+    reference's single-point branch); PSFs and tails as for any site."""
+    from oracle import optics as O
+    from maomi_b200.fixed import run_stage
+    d, cfg, raw = small
+    pt = np.asarray(d["points"])[:1]
+    out = run_stage(cfg, raw, pt, precision="fp64")
+    u64 = O.pupil(cfg, np.float64)
+    ref = O.propagate(cfg, [np.asarray(a, np.float64) for a in raw], pt, u64)
+    for key in ("psf_3d", "psf", "mask_raw", "energies"):
+        assert rel_l2(out[key], ref[key]) < TOL, key
+    assert np.allclose(out["mask_raw"], out["mask_raw"].flat[0])
+    for t in ("psfT", "psfB"):
+        assert rel_l2(out[t]["convmask"], ref[t]["convmask"]) < TOL
