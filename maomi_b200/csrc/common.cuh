@@ -65,8 +65,7 @@ template <bool TW>
 struct __align__(8) cfx_t {
   float x, y;
 };
-using cfx = cfx_t<true>;   // rotations and twiddle tables compensated
-using cfr = cfx_t<false>;  // rotations compensated, FP32 twiddle tables
+using cfx = cfx_t<true>;  // rotations and twiddle tables compensated
 template <class C> struct IsCompensated { static constexpr bool value = false; };
 template <bool TW> struct IsCompensated<cfx_t<TW>> { static constexpr bool value = true; };
 
@@ -99,13 +98,11 @@ template <class C> __device__ __forceinline__ C make_c(double re, double im);
 template <> __device__ __forceinline__ float2 make_c<float2>(double re, double im) { return make_float2(float(re), float(im)); }
 template <> __device__ __forceinline__ double2 make_c<double2>(double re, double im) { return make_double2(re, im); }
 template <> __device__ __forceinline__ cfx from_f2<cfx>(float2 a) { return cfx{a.x, a.y}; }
-template <> __device__ __forceinline__ cfr from_f2<cfr>(float2 a) { return cfr{a.x, a.y}; }
 template <bool TW> __device__ __forceinline__ float2 to_f2(cfx_t<TW> a) { return make_float2(a.x, a.y); }
 template <class C, bool TW> __device__ __forceinline__ C promote(cfx_t<TW> a) { return a; }
 // Twiddle-table entries of a register type: cfx keeps {hi, lo} pairs.
 template <class C> struct TwiddleOf { using T = C; };
 template <> struct TwiddleOf<cfx> { using T = float4; };
-template <> struct TwiddleOf<cfr> { using T = float2; };
 template <class T> __device__ __forceinline__ T make_tw(double re, double im) { return make_c<T>(re, im); }
 template <> __device__ __forceinline__ float4 make_tw<float4>(double re, double im) {
   const float hx = float(re), hy = float(im);

@@ -18,6 +18,7 @@
 #include <type_traits>
 
 #include "common.cuh"
+#include "packed.cuh"
 
 namespace mm {
 
@@ -40,6 +41,12 @@ template <class C> struct Real;
 template <> struct Real<float2> { using T = float; };
 template <> struct Real<double2> { using T = double; };
 template <bool TW> struct Real<cfx_t<TW>> { using T = float; };
+template <> struct Real<cpk> { using T = float; };
+
+__device__ __forceinline__ float2 cneg(float2 a) { return make_float2(-a.x, -a.y); }
+__device__ __forceinline__ double2 cneg(double2 a) { return make_double2(-a.x, -a.y); }
+template <bool TW>
+__device__ __forceinline__ cfx_t<TW> cneg(cfx_t<TW> a) { return cfx_t<TW>{-a.x, -a.y}; }
 
 // a * W_32^k with W = exp(SIGN * 2*pi*i/32), k = 0..15 (angle pi*k/16).
 template <int SIGN, int K, class C>
@@ -49,6 +56,17 @@ __device__ __forceinline__ C rot32(C a) {
     return a;
   } else if constexpr (K == 8) {
     return quarter<SIGN>(a);
+  } else if constexpr (std::is_same_v<C, cpk>) {
+    // packed (re, im), constants as hi + lo float pairs (see cmul_hl)
+    constexpr double c = kCos16[K], s = SIGN * kSin16[K];
+    constexpr float ch = float(c), sh = float(s);
+    constexpr float cl = float(c - double(ch)), sl = float(s - double(sh));
+    if constexpr (K == 4 || K == 12) {
+      constexpr float g = c > 0 ? ch : -ch, gl = c > 0 ? cl : -cl;
+      return cmul_diag(a, c > 0 ? 1.f : -1.f, s > 0 ? 1.f : -1.f, g, gl);
+    } else {
+      return cmul_hl(a, ch, sh, cl, sl);
+    }
   } else if constexpr (IsCompensated<C>::value) {
     // constants as hi + lo float pairs (see cfx)
     constexpr double c = kCos16[K], s = SIGN * kSin16[K];
@@ -129,10 +147,7 @@ __device__ __forceinline__ void dft16(C* v) {
   v[3 + 4 * 1] = rot32<SIGN, 6>(v[3 + 4 * 1]);
   v[3 + 4 * 2] = rot32<SIGN, 12>(v[3 + 4 * 2]);
   {  // W_16^9 = -W_16^1
-    C a = rot32<SIGN, 2>(v[3 + 4 * 3]);
-    a.x = -a.x;
-    a.y = -a.y;
-    v[3 + 4 * 3] = a;
+    v[3 + 4 * 3] = cneg(rot32<SIGN, 2>(v[3 + 4 * 3]));
   }
   // X[k1 + 4*k2] = DFT4 over r of the twiddled F_r[k1]: rows of 4.
 #pragma unroll
@@ -201,9 +216,10 @@ __device__ __forceinline__ void dft(C* v) {
 // exchange suffices.
 //
 // CF / CI are the register arithmetic types of the forward and the inverse
-// half: float2 (FP32), cfr / cfx (FP32 butterflies, rotation constants as
-// hi + lo pairs; cfx also the twiddle tables) or double2 (FP64 butterflies,
-// twiddles and filter).
+// half: float2 (FP32), cpk (FP32 on the packed .f32x2 instructions, rotation
+// constants as hi + lo pairs, FP32 twiddle tables), cfx (scalar FP32,
+// rotations and twiddle tables as hi + lo pairs) or double2 (FP64
+// butterflies, twiddles and filter).
 // The line enters and leaves as complex64 and the exchanges are complex64.
 // The inverse half carries most of the rounding that reaches the saved
 // intensities, so <float2, double2> ("mixed") recovers most of the FP64
@@ -228,6 +244,7 @@ struct FftLine {
   static constexpr int kStrideResidue = R2 == 16 ? 2 : (R1 == 8 ? (R2 == 8 ? 10 : 9) : 3);
   static constexpr int XBUF = R1 * PITCH + ((kStrideResidue - (R1 * PITCH) % 16) + 16) % 16;
   static constexpr bool kFft = true;
+  using XT = float2;
   static constexpr size_t kTwiddleBytes = (size_t)N * (sizeof(TF) + sizeof(TI));
   // CTAs of 128 threads resident per SM the kernels are compiled for: the
   // FP32 forms fit in 80 registers (6 CTAs); FP64 halves need the 4-CTA budget.
@@ -312,6 +329,7 @@ struct DenseLine {
   static constexpr int N = RMAX * 16;  // capacity
   static constexpr int XBUF = N + 1;  // odd stride: lines start on different banks
   static constexpr bool kFft = false;
+  using XT = float2;
   static constexpr int kMinBlocks = RMAX > 16 ? 2 : 4;
 
   template <bool SINGLE = false>

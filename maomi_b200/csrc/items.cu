@@ -289,7 +289,7 @@ extern "C" int mm_propagate_items(const mm_item_class* c, void* workspace, size_
   int rc;
   if (c->precision == MM_PRECISION_FP64) rc = ilaunch_any<double2, double2>(p, c->shape, s);
   else if (c->precision == MM_PRECISION_MIXED) rc = ilaunch_any<float2, double2>(p, c->shape, s);
-  else if (c->precision == MM_PRECISION_COMPENSATED) rc = ilaunch_any<cfr, cfr>(p, c->shape, s);
+  else if (c->precision == MM_PRECISION_COMPENSATED) rc = ilaunch_any<cpk, cpk>(p, c->shape, s);
   else if (c->precision == MM_PRECISION_COMPENSATED_FULL) rc = ilaunch_any<cfx, cfx>(p, c->shape, s);
   else rc = ilaunch_any<float2, float2>(p, c->shape, s);
   if (rc != MM_OK || !check) return rc;

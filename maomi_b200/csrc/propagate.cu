@@ -207,11 +207,16 @@ __device__ void process(const Params& p, const Item& it, float2* xa, float2* xb,
       }
     }
   }
-  // ---------------------------------------- second half of step k-1
   // Row layout keeps each line inside one warp: its exchanges need only warp barriers.
   const bool warp_local = L::kFft && axis == 0 && 32 % R2 == 0;
-  if (it.k > 0)
-    L::template propagate<true>(v, t, st.kern + (size_t)(it.k - 1) * N, N, xa_l, xb_l, twf, twi, warp_local);
+  // Two half-steps share one copy of the line propagator (half 0: second
+  // half of step k-1; half 1: first half of step k), the screen and the
+  // plane save between them: one unrolled transform in the instruction stream.
+#pragma unroll 1
+  for (int half = 0; half < 2; ++half) {
+  if (half == 0 ? it.k > 0 : it.k < st.steps)
+    L::template propagate<true>(v, t, st.kern + (size_t)(it.k - 1 + half) * N, N, xa_l, xb_l, twf, twi, warp_local);
+  if (half == 1) break;
   // ------------------------------------------------------- screen of step k
   if (it.k < st.steps) {
     // the screen samples at the site's window offset, read straight from the
@@ -274,9 +279,7 @@ __device__ void process(const Params& p, const Item& it, float2* xa, float2* xb,
       }
     }
   }
-  // ---------------------------------------- first half of step k
-  if (it.k < st.steps)
-    L::template propagate<true>(v, t, st.kern + (size_t)it.k * N, N, xa_l, xb_l, twf, twi, warp_local);
+  }
   // ------------------------------------------------------------------ store
   if (!(it.stage == 2 && it.k == st.steps)) {
     float2* dst = (it.stage == 1 ? p.bufB + (size_t)it.slot * p.n2 * p.n2 : p.bufA + (size_t)it.slot * p.n * p.n) +
@@ -289,19 +292,25 @@ __device__ void process(const Params& p, const Item& it, float2* xa, float2* xb,
 
 template <class L, int LINES>
 struct Smem {
-  static constexpr size_t xbuf = (size_t)LINES * L::XBUF;     // float2 per exchange buffer (even count)
-  static constexpr size_t bytes = (xbuf + xbuf % 2) * sizeof(float2) + L::kTwiddleBytes + 32 * sizeof(float);
+  static constexpr size_t xbuf = (size_t)LINES * L::XBUF;  // exchange-buffer elements (L::XT)
+  static constexpr size_t xbytes = (xbuf * sizeof(typename L::XT) + 15) / 16 * 16;
+  static constexpr size_t bytes = xbytes + L::kTwiddleBytes + 32 * sizeof(float);
 };
 
 template <class L, int LINES>
 __global__ void __launch_bounds__(LINES * L::R2, L::kMinBlocks * 128 / (LINES * L::R2)) persistent_kernel(Params p) {
   extern __shared__ float4 smem_raw[];
-  float2* xa = reinterpret_cast<float2*>(smem_raw);
-  float2* xb = xa;
-  auto* twf = reinterpret_cast<typename L::TF*>(xa + Smem<L, LINES>::xbuf + Smem<L, LINES>::xbuf % 2);
+  auto* xa = reinterpret_cast<typename L::XT*>(smem_raw);
+  auto* xb = xa;
+  auto* twf = reinterpret_cast<typename L::TF*>(reinterpret_cast<char*>(smem_raw) + Smem<L, LINES>::xbytes);
   auto* twi = reinterpret_cast<typename L::TI*>(reinterpret_cast<char*>(twf) + (L::kFft ? L::N * sizeof(typename L::TF) : 0));
   float* red = reinterpret_cast<float*>(reinterpret_cast<char*>(twi) + (L::kFft ? L::N * sizeof(typename L::TI) : 0));
+  // The queue position and its decoded item live in shared memory: thread 0
+  // claims, decodes (64-bit divisions) and waits for each item once for the
+  // whole CTA, so an item costs two CTA barriers.
   __shared__ long long s_item;
+  __shared__ Item s_it;
+  __shared__ int s_live;
   __shared__ int s_abort;
   if (p.reserve_sms > 0) {
     unsigned sm;
@@ -309,48 +318,65 @@ __global__ void __launch_bounds__(LINES * L::R2, L::kMinBlocks * 128 / (LINES * 
     if (sm < unsigned(p.reserve_sms)) return;  // uniform per CTA; no item claimed yet
   }
   fill_twiddles<L>(twf, twi);
-  if (threadIdx.x == 0) s_item = (long long)atomicAdd(p.head, 1u);
+  // counter value that publishes the segment before item it
+  auto needed = [&](const Item& it) {
+    const StageP& st = p.st[it.stage];
+    return unsigned(it.wave * p.blocks_per_site + st.cum0 + (long long)it.k * st.nblocks);
+  };
+  // thread 0: wait (bounded) until the item's inputs are published
+  auto wait_for = [&](const Item& it) {
+    const unsigned need = needed(it);
+    long long spins = 0;
+    unsigned ns = 32;
+    while (ld_acquire(p.counters + it.slot) < need) {
+      if (++spins > kSpinLimit || (ld_acquire(reinterpret_cast<unsigned*>(p.error)) & 1u) != 0u) {
+        atomicOr(p.error, 1);
+        return 1;
+      }
+      __nanosleep(ns);
+      ns = ns < 256 ? ns * 2 : 256;
+    }
+    return 0;
+  };
+  if (threadIdx.x == 0) {
+    Item it{};
+    s_item = (long long)atomicAdd(p.head, 1u);
+    s_live = s_item < p.total_items ? decode(p, s_item, it) : 0;
+    s_abort = s_live ? wait_for(it) : 0;
+    s_it = it;
+  }
   __syncthreads();
   while (true) {
     const long long item = s_item;
-    if (item >= p.total_items) break;
+    if (item >= p.total_items || s_abort) break;
     // Claim the next item now; the value is only consumed at the end of this
     // one, so the atomic's round trip overlaps the work below.
     unsigned next = 0;
     if (threadIdx.x == 0) next = atomicAdd(p.head, 1u);
-    Item it;
-    const bool live = decode(p, item, it);
-    if (live) {
-      if (threadIdx.x == 0) {
-        const StageP& st = p.st[it.stage];
-        const unsigned need = unsigned(it.wave * p.blocks_per_site + st.cum0 + (long long)it.k * st.nblocks);
-        long long spins = 0;
-        unsigned ns = 32;
-        int abort = 0;
-        while (ld_acquire(p.counters + it.slot) < need) {
-          if (++spins > kSpinLimit || (ld_acquire(reinterpret_cast<unsigned*>(p.error)) & 1u) != 0u) {
-            atomicOr(p.error, 1);
-            abort = 1;
-            break;
-          }
-          __nanosleep(ns);
-          ns = ns < 256 ? ns * 2 : 256;
-        }
-        s_abort = abort;
-      }
-      __syncthreads();
-      if (s_abort) break;
-      process<L, LINES>(p, it, xa, xb, twf, twi, red);
-      __syncthreads();
-      if (threadIdx.x == 0) {
+    const Item it = s_it;
+    const bool live = s_live != 0;
+    if (live) process<L, LINES>(p, it, xa, xb, twf, twi, red);
+    // thread 0 decodes the next item and looks once at its dependency while
+    // the other warps finish
+    Item nit{};
+    int nlive = 0, ready = 0;
+    if (threadIdx.x == 0) {
+      nlive = (long long)next < p.total_items ? int(decode(p, next, nit)) : 0;
+      ready = !nlive || ld_acquire(p.counters + nit.slot) >= needed(nit);
+    }
+    __syncthreads();  // the item's stores are issued and every thread has read s_*
+    if (threadIdx.x == 0) {
+      if (live) {
         // release: the CTA's field stores (ordered by the barrier) become
         // visible before the counter that publishes them
         asm volatile("fence.acq_rel.gpu;" ::: "memory");
         atomicAdd(p.counters + it.slot, 1u);
       }
+      s_abort = ready ? 0 : wait_for(nit);
+      s_item = (long long)next;
+      s_it = nit;
+      s_live = nlive;
     }
-    __syncthreads();  // every thread has read s_item
-    if (threadIdx.x == 0) s_item = (long long)next;
     __syncthreads();
   }
 }
@@ -360,7 +386,7 @@ __global__ void __launch_bounds__(LINES * L::R2, L::kMinBlocks * 128 / (LINES * 
   extern __shared__ float4 smem_raw[];
   float2* xa = reinterpret_cast<float2*>(smem_raw);
   float2* xb = xa;
-  auto* twf = reinterpret_cast<typename L::TF*>(xa + Smem<L, LINES>::xbuf + Smem<L, LINES>::xbuf % 2);
+  auto* twf = reinterpret_cast<typename L::TF*>(reinterpret_cast<char*>(smem_raw) + Smem<L, LINES>::xbytes);
   auto* twi = reinterpret_cast<typename L::TI*>(reinterpret_cast<char*>(twf) + (L::kFft ? L::N * sizeof(typename L::TF) : 0));
   float* red = reinterpret_cast<float*>(reinterpret_cast<char*>(twi) + (L::kFft ? L::N * sizeof(typename L::TI) : 0));
   fill_twiddles<L>(twf, twi);
@@ -462,7 +488,7 @@ int launch_batched_any(Params& p, int stage, int k, int site0, int batch, cudaSt
     case 512:
       if (p.precision == MM_PRECISION_FP64) return launch_batched_fft<double2, double2>(p, stage, k, site0, batch, s);
       if (p.precision == MM_PRECISION_MIXED) return launch_batched_fft<float2, double2>(p, stage, k, site0, batch, s);
-      if (p.precision == MM_PRECISION_COMPENSATED) return launch_batched_fft<cfr, cfr>(p, stage, k, site0, batch, s);
+      if (p.precision == MM_PRECISION_COMPENSATED) return launch_batched_fft<cpk, cpk>(p, stage, k, site0, batch, s);
       if (p.precision == MM_PRECISION_COMPENSATED_FULL) return launch_batched_fft<cfx, cfx>(p, stage, k, site0, batch, s);
       return launch_batched_fft<float2, float2>(p, stage, k, site0, batch, s);
     default:
@@ -508,7 +534,7 @@ int launch_persistent_any(Params& p, cudaStream_t s) {
   }
   if (p.precision == MM_PRECISION_FP64) return launch_persistent_fft<double2, double2>(p, s);
   if (p.precision == MM_PRECISION_MIXED) return launch_persistent_fft<float2, double2>(p, s);
-  if (p.precision == MM_PRECISION_COMPENSATED) return launch_persistent_fft<cfr, cfr>(p, s);
+  if (p.precision == MM_PRECISION_COMPENSATED) return launch_persistent_fft<cpk, cpk>(p, s);
   if (p.precision == MM_PRECISION_COMPENSATED_FULL) return launch_persistent_fft<cfx, cfx>(p, s);
   return launch_persistent_fft<float2, float2>(p, s);
 }
