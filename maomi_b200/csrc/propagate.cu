@@ -251,15 +251,29 @@ __device__ void process(const Params& p, const Item& it, float2* xa, float2* xb,
       // the line must cross the centred n2 crop; then test the in-line coordinate
       const int lc = line - p.crop0;
       if (live && lc >= 0 && lc < p.n2) {
+        // the line's pixel j sits at img0 + ec * estep; the earlier sums of
+        // a group of pixels are read together (one round trip per group),
+        // then the new ones written
+        float* img0 = img + (axis == 0 ? (size_t)lc * p.n2 : (size_t)lc);
+        const size_t estep = axis == 0 ? 1 : (size_t)p.n2;
+        constexpr int G = R1 < 4 ? R1 : 4;
 #pragma unroll
-        for (int j = 0; j < R1; ++j) {
-          const int ec = t + R2 * j - p.crop0;
-          if (!in_line(t + R2 * j) || ec < 0 || ec >= p.n2) continue;
-          const float pw = photon_power(v[j], p.order);
-          psum += pw;
-          float* dst = img + (axis == 0 ? (size_t)lc * p.n2 + ec : (size_t)ec * p.n2 + lc);
-          const float prev = init ? 0.f : __ldcg(dst);
-          __stcg(dst, prev + wgt * pw);
+        for (int g = 0; g < R1; g += G) {
+          float prev[G];
+#pragma unroll
+          for (int i = 0; i < G; ++i) {
+            const int ec = t + R2 * (g + i) - p.crop0;
+            const bool in = in_line(t + R2 * (g + i)) && ec >= 0 && ec < p.n2;
+            prev[i] = (in && !init) ? __ldcg(img0 + (size_t)ec * estep) : 0.f;
+          }
+#pragma unroll
+          for (int i = 0; i < G; ++i) {
+            const int ec = t + R2 * (g + i) - p.crop0;
+            if (!in_line(t + R2 * (g + i)) || ec < 0 || ec >= p.n2) continue;
+            const float pw = photon_power(v[g + i], p.order);
+            psum += pw;
+            __stcg(img0 + (size_t)ec * estep, prev[i] + wgt * pw);
+          }
         }
       }
       const float tot = block_sum(psum, red);
