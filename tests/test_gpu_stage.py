@@ -95,7 +95,7 @@ def test_benchmark_geometry_matches_reference_fp64(bench_sites, precision):
     All-FP32 line transforms sit at ~1.2e-5 here: the rounding of the DFT
     rotation constants is the same in all 240 line transforms of a site, so
     it adds up coherently.  Carrying those constants as hi + lo float pairs
-    (compensated: 1.7e-6; with the twiddle tables too, compensated-full:
+    (compensated: 1.8e-6; with the twiddle tables too, compensated-full:
     4.6e-7), the inverse half in FP64 (mixed: 6e-6) or everything in FP64
     stays inside 1e-5."""
     from maomi_b200.backends.cuda.batched import OpticalPlan
