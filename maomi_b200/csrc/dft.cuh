@@ -245,14 +245,36 @@ struct FftLine {
   static constexpr int XBUF = R1 * PITCH + ((kStrideResidue - (R1 * PITCH) % 16) + 16) % 16;
   static constexpr bool kFft = true;
   using XT = float2;
-  static constexpr size_t kTwiddleBytes = (size_t)N * (sizeof(TF) + sizeof(TI));
+  // Packed halves (cpk) keep one twiddle table: the inverse twiddles are the
+  // conjugates of the forward ones (the same rounded values), read
+  // transposed from rows of R2 + 1 entries (odd pitch: conflict-free both
+  // ways); the shared memory saved stays with L1.
+  static constexpr bool kConjTw = std::is_same_v<CF, cpk> && std::is_same_v<CI, cpk>;
+  static constexpr int TWP = kConjTw ? R2 + 1 : R2;  // pitch of the forward table's rows
+  static constexpr size_t kTwiddleBytes =
+      kConjTw ? (size_t)R1 * TWP * sizeof(TF) : (size_t)N * (sizeof(TF) + sizeof(TI));
   // CTAs of 128 threads resident per SM the kernels are compiled for: the
   // FP32 forms fit in 80 registers (6 CTAs); FP64 halves need the 4-CTA budget.
   static constexpr int kMinBlocks =
       R1 > 16 ? 2 : ((std::is_same_v<CF, double2> || std::is_same_v<CI, double2>) ? 4 : 6);
   static_assert(R1 % R2 == 0, "R2 must divide R1");
 
-  // twf[k1*R2 + t] = W_N^(t*k1) (CF);  twi[n*R1 + k1] = W_N^(-n*k1) (CI).
+  // twf[k1*TWP + t] = W_N^(t*k1) (CF);  twi[n*R1 + k1] = W_N^(-n*k1) (CI),
+  // each formed in FP64 and rounded once.
+  __device__ static void fill_twiddles(TF* twf, TI* twi) {
+    for (int i = threadIdx.x; i < N; i += blockDim.x) {
+      double s, c;
+      const int k1 = i / R2, t = i % R2;
+      sincospi(-2.0 * double((t * k1) % N) / N, &s, &c);
+      twf[k1 * TWP + t] = make_tw<TF>(c, s);
+      if constexpr (!kConjTw) {
+        const int nn = i / R1, kk = i % R1;
+        sincospi(2.0 * double((nn * kk) % N) / N, &s, &c);
+        twi[i] = make_tw<TI>(c, s);
+      }
+    }
+  }
+
   // SINGLE: xa and xb are the same buffer; two more barriers keep the
   // exchanges apart (and the next call's first exchange after this one's last).
   // warp_local: the line's R2 threads share one warp (row layout), so a warp
@@ -270,7 +292,7 @@ struct FftLine {
     // ---- forward pass 1: DFT over m of x[t + R2*m], twiddle, exchange
     dft<R1, -1>(v);
 #pragma unroll
-    for (int k1 = 1; k1 < R1; ++k1) v[k1] = cmul(v[k1], twf[k1 * R2 + t]);
+    for (int k1 = 1; k1 < R1; ++k1) v[k1] = cmul(v[k1], twf[k1 * TWP + t]);
 #pragma unroll
     for (int k1 = 0; k1 < R1; ++k1) xa[k1 * PITCH + t] = to_f2(v[k1]);
     sync();
@@ -298,7 +320,11 @@ struct FftLine {
       for (int na = 0; na < R2; ++na) {
         const int k1 = t + R2 * j;
         CI z = w[j * R2 + na];
-        if (na) z = cmul(z, twi[na * R1 + k1]);
+        if constexpr (kConjTw) {
+          if (na) z = cmul_conj(z, twf[k1 * TWP + na]);
+        } else {
+          if (na) z = cmul(z, twi[na * R1 + k1]);
+        }
         xb[k1 * PITCH + na] = to_f2(z);
       }
     sync();
@@ -329,8 +355,10 @@ struct DenseLine {
   static constexpr int N = RMAX * 16;  // capacity
   static constexpr int XBUF = N + 1;  // odd stride: lines start on different banks
   static constexpr bool kFft = false;
+  static constexpr bool kConjTw = false;
   using XT = float2;
   static constexpr int kMinBlocks = RMAX > 16 ? 2 : 4;
+  __device__ static void fill_twiddles(TF*, TI*) {}
 
   template <bool SINGLE = false>
   __device__ static void propagate(float2 (&v)[R1], int t, const float2* __restrict__ ker, int n, float2* xa,

@@ -67,30 +67,17 @@ struct ISmem {
   static constexpr size_t bytes = (xbuf + xbuf % 2) * sizeof(float2) + L::kTwiddleBytes + screen * sizeof(float);
 };
 
-template <class L>
-__device__ void ifill_twiddles(typename L::TF* twf, typename L::TI* twi) {
-  for (int i = threadIdx.x; i < L::N; i += blockDim.x) {
-    double s, c;
-    const int k1 = i / L::R2, t = i % L::R2;
-    sincospi(-2.0 * double((t * k1) % L::N) / L::N, &s, &c);
-    twf[i] = make_tw<typename L::TF>(c, s);
-    const int nn = i / L::R1, k2 = i % L::R1;
-    sincospi(2.0 * double((nn * k2) % L::N) / L::N, &s, &c);
-    twi[i] = make_tw<typename L::TI>(c, s);
-  }
-}
-
 template <class L, int LINES>
 __global__ void __launch_bounds__(LINES * L::R2, L::kMinBlocks * 128 / (LINES * L::R2)) items_kernel(ItemP p) {
   constexpr int R1 = L::R1, R2 = L::R2, N = L::N;
   extern __shared__ float4 smem_raw[];
   float2* xa = reinterpret_cast<float2*>(smem_raw);
   auto* twf = reinterpret_cast<typename L::TF*>(xa + ISmem<L, LINES>::xbuf + ISmem<L, LINES>::xbuf % 2);
-  auto* twi = reinterpret_cast<typename L::TI*>(twf + N);
-  float* ph_s = reinterpret_cast<float*>(twi + N);
+  auto* twi = reinterpret_cast<typename L::TI*>(reinterpret_cast<char*>(twf) + (L::kConjTw ? 0 : N * sizeof(typename L::TF)));
+  float* ph_s = reinterpret_cast<float*>(reinterpret_cast<char*>(twf) + L::kTwiddleBytes);
   __shared__ long long s_item;
   __shared__ int s_abort;
-  ifill_twiddles<L>(twf, twi);
+  L::fill_twiddles(twf, twi);
   if (threadIdx.x == 0) s_item = (long long)atomicAdd(p.head, 1u);
   __syncthreads();
   while (true) {

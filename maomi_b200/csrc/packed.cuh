@@ -39,6 +39,10 @@ __device__ __forceinline__ cpk quarter(cpk a) {
 __device__ __forceinline__ cpk cmul(cpk a, float2 w) {
   return pk(__ffma2_rn(f2(a), bc(w.x), __fmul2_rn(swapped(a), make_float2(-w.y, w.y))));
 }
+// a * conj(w)
+__device__ __forceinline__ cpk cmul_conj(cpk a, float2 w) {
+  return pk(__ffma2_rn(f2(a), bc(w.x), __fmul2_rn(swapped(a), make_float2(w.y, -w.y))));
+}
 // a * (hi + lo) for a rotation constant (c, s) given as hi + lo float pairs
 __device__ __forceinline__ cpk cmul_hl(cpk a, float ch, float sh, float cl, float sl) {
   const float2 lo = __ffma2_rn(f2(a), bc(cl), __fmul2_rn(swapped(a), make_float2(-sl, sl)));

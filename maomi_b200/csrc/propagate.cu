@@ -105,26 +105,6 @@ __device__ __forceinline__ float block_sum(float v, float* red) {
   return s;  // valid in thread 0
 }
 
-// Twiddle tables for an N = R1*R2 line, in FP64 rounded once to float.
-template <class L>
-__device__ void fill_twiddles(typename L::TF* twf, typename L::TI* twi) {
-  if constexpr (!L::kFft) return;
-  for (int i = threadIdx.x; i < L::N; i += blockDim.x) {
-    {  // twf[k1*R2 + t] = exp(-2 pi i t k1 / N)
-      const int k1 = i / L::R2, t = i % L::R2;
-      double s, c;
-      sincospi(-2.0 * double((t * k1) % L::N) / L::N, &s, &c);
-      twf[i] = make_tw<typename L::TF>(c, s);
-    }
-    {  // twi[n*R1 + k1] = exp(+2 pi i n k1 / N)
-      const int nn = i / L::R1, k1 = i % L::R1;
-      double s, c;
-      sincospi(2.0 * double((nn * k1) % L::N) / L::N, &s, &c);
-      twi[i] = make_tw<typename L::TI>(c, s);
-    }
-  }
-}
-
 // Which line of the item this thread works on, and its place in the line:
 // rows (axis 0) keep a line's threads in one warp; columns (axis 1) put 32
 // consecutive columns in a warp so every global access is a full segment.
@@ -304,21 +284,35 @@ __device__ void process(const Params& p, const Item& it, float2* xa, float2* xb,
   }
 }
 
+// Dynamic shared memory of a propagation CTA: the exchange buffer, the
+// twiddle tables and the reduction scratch.  More shared memory (a second
+// exchange buffer, staged screens) measured slower: it comes out of L1.
 template <class L, int LINES>
 struct Smem {
   static constexpr size_t xbuf = (size_t)LINES * L::XBUF;  // exchange-buffer elements (L::XT)
   static constexpr size_t xbytes = (xbuf * sizeof(typename L::XT) + 15) / 16 * 16;
   static constexpr size_t bytes = xbytes + L::kTwiddleBytes + 32 * sizeof(float);
+  struct Parts {
+    typename L::XT* xa;
+    typename L::TF* twf;
+    typename L::TI* twi;
+    float* red;
+  };
+  __device__ static Parts carve(void* base) {
+    char* b = static_cast<char*>(base);
+    Parts q;
+    q.xa = reinterpret_cast<typename L::XT*>(b);
+    q.twf = reinterpret_cast<typename L::TF*>(b + xbytes);
+    q.twi = reinterpret_cast<typename L::TI*>(b + xbytes + (L::kConjTw ? 0 : L::N * sizeof(typename L::TF)));
+    q.red = reinterpret_cast<float*>(b + xbytes + L::kTwiddleBytes);
+    return q;
+  }
 };
 
 template <class L, int LINES>
 __global__ void __launch_bounds__(LINES * L::R2, L::kMinBlocks * 128 / (LINES * L::R2)) persistent_kernel(Params p) {
   extern __shared__ float4 smem_raw[];
-  auto* xa = reinterpret_cast<typename L::XT*>(smem_raw);
-  auto* xb = xa;
-  auto* twf = reinterpret_cast<typename L::TF*>(reinterpret_cast<char*>(smem_raw) + Smem<L, LINES>::xbytes);
-  auto* twi = reinterpret_cast<typename L::TI*>(reinterpret_cast<char*>(twf) + (L::kFft ? L::N * sizeof(typename L::TF) : 0));
-  float* red = reinterpret_cast<float*>(reinterpret_cast<char*>(twi) + (L::kFft ? L::N * sizeof(typename L::TI) : 0));
+  const auto sm = Smem<L, LINES>::carve(smem_raw);
   // The queue position and its decoded item live in shared memory: thread 0
   // claims, decodes (64-bit divisions) and waits for each item once for the
   // whole CTA, so an item costs two CTA barriers.
@@ -327,11 +321,11 @@ __global__ void __launch_bounds__(LINES * L::R2, L::kMinBlocks * 128 / (LINES * 
   __shared__ int s_live;
   __shared__ int s_abort;
   if (p.reserve_sms > 0) {
-    unsigned sm;
-    asm volatile("mov.u32 %0, %%smid;" : "=r"(sm));
-    if (sm < unsigned(p.reserve_sms)) return;  // uniform per CTA; no item claimed yet
+    unsigned smid;
+    asm volatile("mov.u32 %0, %%smid;" : "=r"(smid));
+    if (smid < unsigned(p.reserve_sms)) return;  // uniform per CTA; no item claimed yet
   }
-  fill_twiddles<L>(twf, twi);
+  L::fill_twiddles(sm.twf, sm.twi);
   // counter value that publishes the segment before item it
   auto needed = [&](const Item& it) {
     const StageP& st = p.st[it.stage];
@@ -369,7 +363,7 @@ __global__ void __launch_bounds__(LINES * L::R2, L::kMinBlocks * 128 / (LINES * 
     if (threadIdx.x == 0) next = atomicAdd(p.head, 1u);
     const Item it = s_it;
     const bool live = s_live != 0;
-    if (live) process<L, LINES>(p, it, xa, xb, twf, twi, red);
+    if (live) process<L, LINES>(p, it, sm.xa, sm.xa, sm.twf, sm.twi, sm.red);
     // thread 0 decodes the next item and looks once at its dependency while
     // the other warps finish
     Item nit{};
@@ -398,12 +392,8 @@ __global__ void __launch_bounds__(LINES * L::R2, L::kMinBlocks * 128 / (LINES * 
 template <class L, int LINES>
 __global__ void __launch_bounds__(LINES * L::R2, L::kMinBlocks * 128 / (LINES * L::R2)) batched_kernel(Params p) {
   extern __shared__ float4 smem_raw[];
-  float2* xa = reinterpret_cast<float2*>(smem_raw);
-  float2* xb = xa;
-  auto* twf = reinterpret_cast<typename L::TF*>(reinterpret_cast<char*>(smem_raw) + Smem<L, LINES>::xbytes);
-  auto* twi = reinterpret_cast<typename L::TI*>(reinterpret_cast<char*>(twf) + (L::kFft ? L::N * sizeof(typename L::TF) : 0));
-  float* red = reinterpret_cast<float*>(reinterpret_cast<char*>(twi) + (L::kFft ? L::N * sizeof(typename L::TI) : 0));
-  fill_twiddles<L>(twf, twi);
+  const auto sm = Smem<L, LINES>::carve(smem_raw);
+  L::fill_twiddles(sm.twf, sm.twi);
   __syncthreads();
   const StageP& st = p.st[p.b_stage];
   Item it;
@@ -414,7 +404,7 @@ __global__ void __launch_bounds__(LINES * L::R2, L::kMinBlocks * 128 / (LINES * 
   it.site = p.b_site0 + it.slot;
   it.wave = 0;
   if (it.site >= p.nsites) return;
-  process<L, LINES>(p, it, xa, xb, twf, twi, red);
+  process<L, LINES>(p, it, sm.xa, sm.xa, sm.twf, sm.twi, sm.red);
 }
 
 // ------------------------------------------------------------------- host --
