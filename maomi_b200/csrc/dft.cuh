@@ -277,6 +277,10 @@ struct FftLine {
 
   // SINGLE: xa and xb are the same buffer; two more barriers keep the
   // exchanges apart (and the next call's first exchange after this one's last).
+  // With R1 == R2 they are not needed: thread t reads back exactly the row it
+  // writes next (row t: forward pass 2, then inverse pass 1) and the column
+  // it writes next (column t: inverse pass 2, then the next forward pass 1),
+  // so no thread overwrites a word another thread has still to read.
   // warp_local: the line's R2 threads share one warp (row layout), so a warp
   // barrier orders the exchanges; otherwise the whole CTA synchronises.
   template <bool SINGLE = false>
@@ -313,7 +317,7 @@ struct FftLine {
     // ---- inverse pass 1: IDFT over k2 -> n_a, twiddle W_N^(-n_a*k1), exchange
 #pragma unroll
     for (int j = 0; j < J; ++j) dft<R2, +1>(w + j * R2);
-    if constexpr (SINGLE) sync();  // forward reads of the shared buffer done
+    if constexpr (SINGLE && J > 1) sync();  // forward reads of the shared buffer done
 #pragma unroll
     for (int j = 0; j < J; ++j)
 #pragma unroll
@@ -334,7 +338,7 @@ struct FftLine {
     dft<R1, +1>(w);
 #pragma unroll
     for (int m = 0; m < R1; ++m) x[m] = to_f2(w[m]);
-    if constexpr (SINGLE) sync();  // inverse reads done before the buffer is reused
+    if constexpr (SINGLE && J > 1) sync();  // inverse reads done before the buffer is reused
   }
 };
 
