@@ -246,11 +246,14 @@ struct FftLine {
   static constexpr bool kFft = true;
   using XT = float2;
   // Packed halves (cpk) keep one twiddle table: the inverse twiddles are the
-  // conjugates of the forward ones (the same rounded values), read
-  // transposed from rows of R2 + 1 entries (odd pitch: conflict-free both
-  // ways); the shared memory saved stays with L1.
+  // conjugates of the forward ones (the same rounded values); the shared
+  // memory saved stays with L1.  For R1 == R2 the table W^(t*k) is
+  // symmetric, so it is stored thread-major — row t holds every twiddle
+  // thread t applies in either direction — and read 16 bytes at a time
+  // (rows of R2 + 2 entries: 16-byte aligned, conflict-free).
   static constexpr bool kConjTw = std::is_same_v<CF, cpk> && std::is_same_v<CI, cpk>;
-  static constexpr int TWP = kConjTw ? R2 + 1 : R2;  // pitch of the forward table's rows
+  static constexpr bool kRowTw = kConjTw && R1 == R2;
+  static constexpr int TWP = kRowTw ? R2 + 2 : (kConjTw ? R2 + 1 : R2);  // pitch of the forward table's rows
   static constexpr size_t kTwiddleBytes =
       kConjTw ? (size_t)R1 * TWP * sizeof(TF) : (size_t)N * (sizeof(TF) + sizeof(TI));
   // CTAs of 128 threads resident per SM the kernels are compiled for: the
@@ -266,7 +269,7 @@ struct FftLine {
       double s, c;
       const int k1 = i / R2, t = i % R2;
       sincospi(-2.0 * double((t * k1) % N) / N, &s, &c);
-      twf[k1 * TWP + t] = make_tw<TF>(c, s);
+      twf[k1 * TWP + t] = make_tw<TF>(c, s);  // row k1 = thread-major row t (symmetric) when kRowTw
       if constexpr (!kConjTw) {
         const int nn = i / R1, kk = i % R1;
         sincospi(2.0 * double((nn * kk) % N) / N, &s, &c);
@@ -295,8 +298,18 @@ struct FftLine {
     for (int m = 0; m < R1; ++m) v[m] = from_f2<CF>(x[m]);
     // ---- forward pass 1: DFT over m of x[t + R2*m], twiddle, exchange
     dft<R1, -1>(v);
+    if constexpr (kRowTw) {
+      const float4* row = reinterpret_cast<const float4*>(twf + t * TWP);
 #pragma unroll
-    for (int k1 = 1; k1 < R1; ++k1) v[k1] = cmul(v[k1], twf[k1 * TWP + t]);
+      for (int k = 0; k < R1; k += 2) {
+        const float4 w2 = row[k / 2];
+        if (k) v[k] = cmul(v[k], make_float2(w2.x, w2.y));
+        v[k + 1] = cmul(v[k + 1], make_float2(w2.z, w2.w));
+      }
+    } else {
+#pragma unroll
+      for (int k1 = 1; k1 < R1; ++k1) v[k1] = cmul(v[k1], twf[k1 * TWP + t]);
+    }
 #pragma unroll
     for (int k1 = 0; k1 < R1; ++k1) xa[k1 * PITCH + t] = to_f2(v[k1]);
     sync();
@@ -318,19 +331,32 @@ struct FftLine {
 #pragma unroll
     for (int j = 0; j < J; ++j) dft<R2, +1>(w + j * R2);
     if constexpr (SINGLE && J > 1) sync();  // forward reads of the shared buffer done
+    if constexpr (kRowTw) {  // J == 1, k1 = t: row t, conjugated
+      const float4* row = reinterpret_cast<const float4*>(twf + t * TWP);
 #pragma unroll
-    for (int j = 0; j < J; ++j)
-#pragma unroll
-      for (int na = 0; na < R2; ++na) {
-        const int k1 = t + R2 * j;
-        CI z = w[j * R2 + na];
-        if constexpr (kConjTw) {
-          if (na) z = cmul_conj(z, twf[k1 * TWP + na]);
-        } else {
-          if (na) z = cmul(z, twi[na * R1 + k1]);
-        }
-        xb[k1 * PITCH + na] = to_f2(z);
+      for (int na = 0; na < R2; na += 2) {
+        const float4 w2 = row[na / 2];
+        CI z0 = w[na], z1 = w[na + 1];
+        if (na) z0 = cmul_conj(z0, make_float2(w2.x, w2.y));
+        z1 = cmul_conj(z1, make_float2(w2.z, w2.w));
+        xb[t * PITCH + na] = to_f2(z0);
+        xb[t * PITCH + na + 1] = to_f2(z1);
       }
+    } else {
+#pragma unroll
+      for (int j = 0; j < J; ++j)
+#pragma unroll
+        for (int na = 0; na < R2; ++na) {
+          const int k1 = t + R2 * j;
+          CI z = w[j * R2 + na];
+          if constexpr (kConjTw) {
+            if (na) z = cmul_conj(z, twf[k1 * TWP + na]);
+          } else {
+            if (na) z = cmul(z, twi[na * R1 + k1]);
+          }
+          xb[k1 * PITCH + na] = to_f2(z);
+        }
+    }
     sync();
     // ---- inverse pass 2: thread t = n_a gathers every k1
 #pragma unroll
