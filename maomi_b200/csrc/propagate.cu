@@ -215,7 +215,8 @@ __device__ void process(const Params& p, const Item& it, float2* xa, float2* xb,
       const float w = axis == 0 ? eline * __ldg(st.edge + e) : __ldg(st.edge + e) * eline;
       float2 s = sv[j];
       s = make_float2(s.x * w, s.y * w);
-      v[j] = cmul(v[j], s);
+      if constexpr (std::is_same_v<typename L::CF, cpk>) v[j] = to_f2(cmul(from_f2<cpk>(v[j]), s));  // packed
+      else v[j] = cmul(v[j], s);
     }
   }
   // ------------------------------------------------------------ plane save
