@@ -257,8 +257,10 @@ __device__ void process(const Params& p, const Item& it, float2* xa, float2* xb,
           }
         }
       }
-      const float tot = block_sum(psum, red);
-      if (threadIdx.x == 0) atomicAdd(p.profile[tail] + (size_t)it.site * p.planes[tail] + pt, (double)tot);
+      // the plane's power: warp sums, one FP64 atomic per warp (no CTA barrier)
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) psum += __shfl_xor_sync(0xffffffffu, psum, o);
+      if ((threadIdx.x & 31) == 0) atomicAdd(p.profile[tail] + (size_t)it.site * p.planes[tail] + pt, (double)psum);
     } else if (it.stage == 1 && it.k < st.steps) {
       float* dst = p.focal + ((size_t)it.site * st.steps + it.k) * p.fh * p.fw;
       const int lf = line - (axis == 0 ? p.fx0 : p.fy0);            // line inside the focal crop?
