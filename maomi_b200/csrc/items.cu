@@ -10,6 +10,7 @@
 // the fixed-lattice stage.  Screens are formed from the float32 phase stacks
 // in the kernel (cp.async prefetch, sincosf), so only the phases are stored.
 #include <algorithm>
+#include <type_traits>
 
 #include "common.cuh"
 #include "dft.cuh"
@@ -75,18 +76,46 @@ __global__ void __launch_bounds__(LINES * L::R2, L::kMinBlocks * 128 / (LINES * 
   auto* twf = reinterpret_cast<typename L::TF*>(xa + ISmem<L, LINES>::xbuf + ISmem<L, LINES>::xbuf % 2);
   auto* twi = reinterpret_cast<typename L::TI*>(reinterpret_cast<char*>(twf) + (L::kConjTw ? 0 : N * sizeof(typename L::TF)));
   float* ph_s = reinterpret_cast<float*>(reinterpret_cast<char*>(twf) + L::kTwiddleBytes);
+  // Thread 0 claims, decodes and waits for each item once for the CTA; an
+  // item costs two CTA barriers (as in the fixed-lattice stage kernel).
   __shared__ long long s_item;
+  __shared__ IItem s_it;
+  __shared__ int s_live;
   __shared__ int s_abort;
   L::fill_twiddles(twf, twi);
-  if (threadIdx.x == 0) s_item = (long long)atomicAdd(p.head, 1u);
+  auto needed = [&](IItem it) {
+    return unsigned(p.slot_base[it.wave * p.slots + it.slot] + it.level * p.nblocks);
+  };
+  auto wait_for = [&](IItem it) {
+    const unsigned need = needed(it);
+    long long spins = 0;
+    unsigned ns = 32;
+    while (ld_acquire(p.counters + it.slot) < need) {
+      if (++spins > kItemSpinLimit || (ld_acquire(reinterpret_cast<unsigned*>(p.error)) & 1u) != 0u) {
+        atomicOr(p.error, 1);
+        return 1;
+      }
+      __nanosleep(ns);
+      ns = ns < 256 ? ns * 2 : 256;
+    }
+    return 0;
+  };
+  if (threadIdx.x == 0) {
+    IItem it{};
+    s_item = (long long)atomicAdd(p.head, 1u);
+    s_live = s_item < p.total ? int(idecode(p, s_item, it)) : 0;
+    s_abort = s_live ? wait_for(it) : 0;
+    s_it = it;
+  }
   __syncthreads();
   while (true) {
     const long long q = s_item;
-    if (q >= p.total) break;
+    if (q >= p.total || s_abort) break;
     unsigned next = 0;
     if (threadIdx.x == 0) next = atomicAdd(p.head, 1u);
-    IItem it;
-    if (idecode(p, q, it)) {
+    const IItem it = s_it;
+    const bool live = s_live != 0;
+    if (live) {
       const int S = p.steps[it.item];
       const int axis = it.level & 1;
       const int tid = threadIdx.x;
@@ -95,7 +124,7 @@ __global__ void __launch_bounds__(LINES * L::R2, L::kMinBlocks * 128 / (LINES * 
       const int line = it.block * LINES + line_local;
       const int row0 = axis == 0 ? line : t, col0 = axis == 0 ? t : line;
       const int jstep = axis == 0 ? R2 : R2 * N;
-      // ---- prefetch this thread's phase samples (inputs: before the wait)
+      // ---- this thread's phase samples, copied while the field loads
       if (it.level < S) {
         const float* ph = p.phase + p.phase_off[it.item] + (size_t)it.level * N * N + (size_t)row0 * N + col0;
 #pragma unroll
@@ -105,24 +134,6 @@ __global__ void __launch_bounds__(LINES * L::R2, L::kMinBlocks * 128 / (LINES * 
         }
         cp_async_commit();
       }
-      if (threadIdx.x == 0) {
-        const unsigned need = unsigned(p.slot_base[it.wave * p.slots + it.slot] + it.level * p.nblocks);
-        long long spins = 0;
-        unsigned ns = 32;
-        int abort = 0;
-        while (ld_acquire(p.counters + it.slot) < need) {
-          if (++spins > kItemSpinLimit || (ld_acquire(reinterpret_cast<unsigned*>(p.error)) & 1u) != 0u) {
-            atomicOr(p.error, 1);
-            abort = 1;
-            break;
-          }
-          __nanosleep(ns);
-          ns = ns < 256 ? ns * 2 : 256;
-        }
-        s_abort = abort;
-      }
-      __syncthreads();
-      if (s_abort) break;
       float2* xl = xa + line_local * L::XBUF;
       const bool warp_local = axis == 0 && 32 % R2 == 0;
       float2 v[R1];
@@ -130,8 +141,13 @@ __global__ void __launch_bounds__(LINES * L::R2, L::kMinBlocks * 128 / (LINES * 
       src += (size_t)row0 * N + col0;
 #pragma unroll
       for (int j = 0; j < R1; ++j) v[j] = it.level == 0 ? __ldg(src + (size_t)j * jstep) : __ldcg(src + (size_t)j * jstep);
-      if (it.level > 0) L::template propagate<true>(v, t, p.kern, N, xl, xl, twf, twi, warp_local);
-      if (it.level < S) {
+      // half 0: the second half of step level-1; half 1: the first half of
+      // step level (one unrolled copy of the line propagator)
+#pragma unroll 1
+      for (int half = 0; half < 2; ++half) {
+        if (half == 0 ? it.level > 0 : it.level < S)
+          L::template propagate<true>(v, t, p.kern, N, xl, xl, twf, twi, warp_local);
+        if (half == 1 || it.level >= S) break;
         cp_async_wait_all();
         const float eline = p.edge ? __ldg(p.edge + line) : 1.f;
 #pragma unroll
@@ -144,22 +160,34 @@ __global__ void __launch_bounds__(LINES * L::R2, L::kMinBlocks * 128 / (LINES * 
             cs *= w;
             sn *= w;
           }
-          v[j] = cmul(v[j], make_float2(cs, sn));
+          if constexpr (std::is_same_v<typename L::CF, cpk>) v[j] = to_f2(cmul(from_f2<cpk>(v[j]), make_float2(cs, sn)));
+          else v[j] = cmul(v[j], make_float2(cs, sn));
         }
-        L::template propagate<true>(v, t, p.kern, N, xl, xl, twf, twi, warp_local);
       }
       float2* dst = (it.level == S ? p.field_out + (size_t)it.item * N * N : p.buf + (size_t)it.slot * N * N) +
                     (size_t)row0 * N + col0;
 #pragma unroll
       for (int j = 0; j < R1; ++j) __stcg(dst + (size_t)j * jstep, v[j]);
-      __syncthreads();
-      if (threadIdx.x == 0) {
+    }
+    // thread 0 decodes the next item and looks once at its dependency while
+    // the other warps finish
+    IItem nit{};
+    int nlive = 0, ready = 0;
+    if (threadIdx.x == 0) {
+      nlive = (long long)next < p.total ? int(idecode(p, next, nit)) : 0;
+      ready = !nlive || ld_acquire(p.counters + nit.slot) >= needed(nit);
+    }
+    __syncthreads();  // the item's stores are issued and every thread has read s_*
+    if (threadIdx.x == 0) {
+      if (live) {
         asm volatile("fence.acq_rel.gpu;" ::: "memory");
         atomicAdd(p.counters + it.slot, 1u);
       }
+      s_abort = ready ? 0 : wait_for(nit);
+      s_item = (long long)next;
+      s_it = nit;
+      s_live = nlive;
     }
-    __syncthreads();
-    if (threadIdx.x == 0) s_item = (long long)next;
     __syncthreads();
   }
 }
