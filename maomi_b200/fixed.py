@@ -293,11 +293,19 @@ def run_stages(config, blocks, points_um=None, *, device="cuda", depth=2, return
     import collections
     import torch
     copy = torch.cuda.Stream(device=device)
+    up = torch.cuda.Stream(device=device)
+    main = torch.cuda.current_stream(device)
     pending = collections.deque()
     count = 0
     for raw in blocks:
-        fields = [a.to(device, non_blocking=True) if isinstance(a, torch.Tensor) else _lib.upload(a, device)
-                  for a in raw]
+        # uploads run on their own stream, so block i+1's fields cross PCIe
+        # while block i still computes; the compute stream waits for them
+        with torch.cuda.stream(up):
+            fields = [a.to(device, non_blocking=True) if isinstance(a, torch.Tensor) else _lib.upload(a, device)
+                      for a in raw]
+        main.wait_stream(up)
+        for f in fields:
+            f.record_stream(main)
         dev = stage_device(config, fields, points_um, device=device, **kwargs)
         out = None
         if reuse:
