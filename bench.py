@@ -58,9 +58,10 @@ def parse():
     ap.add_argument("--sites", type=int, default=SITES, help="profile a subset of the lattice (not a bench line)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--precision", default="compensated", choices=["compensated", "compensated-full", "mixed", "fp64", "fp32"])
-    ap.add_argument("--workload", default="stage", choices=["stage", "surrogate", "uneven", "local"],
+    ap.add_argument("--workload", default="stage", choices=["stage", "surrogate", "uneven", "local", "fields"],
                     help="stage: the headline optical stage; surrogate: the learned PSF path with its plain gate; "
-                         "uneven: 6,000 mixed-size items in one graph; local: the local-PSF render")
+                         "uneven: 6,000 mixed-size items in one graph; local: the local-PSF render; "
+                         "fields: the raw A/B/C scattering fields of the benchmark geometry")
     ap.add_argument("--reserve-sms", type=int, default=None,
                     help="SMs the propagation leaves to the overlapped v4 factorisation (default: the library's)")
     ap.add_argument("--train-sites", type=int, default=20000)
@@ -377,12 +378,83 @@ def run_local(args):
           clocks=clk.summary())
 
 
+def run_fields(args):
+    """Scattering-field generation for the benchmark geometry: the three raw
+    A/B/C fields (768 x 768 x 10/46/4 = 35.4 M voxels), noise drawn on the
+    device, spectrum and finish kernels around cuFFT's inverse 3-D DFT."""
+    import torch
+    from maomi_b200 import _lib, synthetic
+    from maomi_b200.fields import field_extents, prepare_fields
+    from maomi_b200.optics import OpticalConfig
+    dev = "cuda:0"
+    torch.cuda.set_device(0)
+    stream = torch.cuda.current_stream(dev)
+    lib = _lib.load()
+    cfg = synthetic.benchmark_stage_config(OpticalConfig)
+    shapes = field_extents(cfg)[0]
+    voxels = int(sum(np.prod(s) for s in shapes))
+    launches0 = lib.mm_launch_count()
+    with Clocks(0) as clk:
+        ms = _timed(lambda: prepare_fields(cfg, device=dev), args.steps, args.warmup, stream)
+    launches = (lib.mm_launch_count() - launches0) / (args.steps + args.warmup)
+    host = [torch.empty(tuple(s), dtype=torch.float32).pin_memory() for s in shapes]
+
+    def to_host():
+        for h, d in zip(host, prepare_fields(cfg, device=dev)):
+            h.copy_(d, non_blocking=True)
+
+    e2e_ms = _timed(to_host, args.steps, 1, stream)
+    # the hand-written spectrum kernel alone on field B: 8 B of noise read and
+    # 8 B of spectrum written per voxel
+    s1 = tuple(int(v) for v in shapes[1])
+    noise = (torch.randn(s1, device=dev), torch.randn(s1, device=dev))
+    ls = np.repeat(np.asarray(cfg.scatter_scales_um, np.float32)[:, None], 3, 1) * np.float32(cfg.vres)
+    spec_ms = _timed_spectrum(s1, ls, cfg.scatter_weights, noise, args.steps, stream)
+    nb = int(np.prod(s1))
+    achieved = 16.0 * nb / (spec_ms * 1e-3) / 1e9
+    pk, pk_kind = peaks()
+    from oracle import fields as OF
+    t0 = time.perf_counter()
+    OF.prepare_fields(cfg, OF.torch_noise(shapes, cfg.seed))
+    t_cpu = time.perf_counter() - t0
+    _line("raw field voxels/s (benchmark A/B/C fields, 768^2 x 60 slabs)", voxels / (ms * 1e-3), "voxels/s", args, ms,
+          {"workload": "prepare_fields, benchmark geometry: 768x768x10 + 768x768x46 + 768x768x4, 4 GP scales",
+           "l2": "fields 141 MB + complex spectra 283 MB: larger than L2"}, dtype="f32",
+          e2e={"value": voxels / (e2e_ms * 1e-3), "unit": "voxels/s", "h2d_bytes_per_step": 0,
+               "d2h_bytes_per_step": int(voxels * 4)},
+          gpu_launches=launches,
+          roofline={"bound": "hbm", "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
+                    "frac": achieved / pk["hbm_gbs"], "traffic": None, "kernel": "mm_gp_spectrum (field B)",
+                    "kernel_ms": spec_ms, "bytes_per_launch": 16 * nb, "peak_source": pk_kind},
+          cpu_baseline={"value": voxels / t_cpu, "unit": "voxels/s", "cores": 1, "kind": "port",
+                        "sample": "the three benchmark fields by the NumPy restatement (torch CPU draws, FP64 FFT)"},
+          clocks=clk.summary())
+
+
+def _timed_spectrum(shape, ls, weights, noise, steps, stream):
+    import torch
+    from maomi_b200 import _lib
+    from maomi_b200.fields import _grid2, _scale_tables
+    dev = noise[0].device
+    g2 = [_grid2(n).to(dev) for n in shape]
+    l2, prod_l, w2, k = _scale_tables(ls, weights, dev)
+    spec = torch.empty(shape, dtype=torch.complex64, device=dev)
+    st = _lib.stream_of(dev)
+
+    def once():
+        _lib.call("mm_gp_spectrum", *shape, _lib.ptr(g2[0]), _lib.ptr(g2[1]), _lib.ptr(g2[2]), k, _lib.ptr(l2),
+                  _lib.ptr(prod_l), _lib.ptr(w2), _lib.ptr(noise[0]), _lib.ptr(noise[1]), _lib.ptr(spec), st)
+
+    return _timed(once, steps, 3, stream)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
     if args.workload != "stage":
-        return {"surrogate": run_surrogate, "uneven": run_uneven, "local": run_local}[args.workload](args)
+        return {"surrogate": run_surrogate, "uneven": run_uneven, "local": run_local,
+                "fields": run_fields}[args.workload](args)
     import torch
     import torch.distributed as dist
     world = int(os.environ.get("WORLD_SIZE", "1"))

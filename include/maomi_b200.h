@@ -317,6 +317,37 @@ int mm_resample_images(const float* in /* (S,H,W) */, int S, int H, int W, const
                        float* out /* (S,X,Y) */, void* stream);
 
 /* ------------------------------------------------------------------------
+ * Scattering-field generation (the stage's raw A/B/C inputs).
+ * Replaces masked_3DGP_test, maomi/_optical_math.py:20-67, and the field
+ * loop of prepare_fields, maomi/optics.py:145-196.  One Gaussian-process
+ * draw is mm_gp_spectrum, an inverse 3-D DFT normalised by 1/N (complex64),
+ * then mm_gp_finish.  Grids are C-ordered (nx, ny, nz).
+ */
+
+/* spec[x,y,z] = (re + i im)[s] * S[s], s = ((x + nx/2) % nx, (y + ny/2) % ny,
+ * (z + nz/2) % nz) (ifftshift), S = sqrt(sum_k prod_l[k] (kx ky kz)^2 w2[k]),
+ * kx = exp(-g2x[sx] * l2[3k]) (and y, z likewise).  g2x/g2y/g2z: the squared
+ * linspace(-pi/2, pi/2, n) grids; l2: squared scales (nscales, 3); prod_l:
+ * l_x l_y l_z; w2: squared weights; noise_re/noise_im: (nx,ny,nz) float32;
+ * spec: complex64 (nx,ny,nz).  All device pointers. */
+int mm_gp_spectrum(int nx, int ny, int nz, const float* g2x, const float* g2y, const float* g2z, int nscales,
+                   const float* l2, const float* prod_l, const float* w2, const float* noise_re,
+                   const float* noise_im, void* spec, void* stream);
+
+/* out[x,y,z] = scale * Re(y[ifftshift(x,y,z)]), times `first` on z = 0 and
+ * `last` on z = nz-1 (the partial-slab factors of optics.py:167-170); scale =
+ * 2 * p_scale * sqrt(nx*ny*nz).  y: complex64 device array, out: float32. */
+int mm_gp_finish(const void* y, int nx, int ny, int nz, float scale, float first, float last, float* out,
+                 void* stream);
+
+/* Vessel occupancy (optics.py:171-196): raw[x,y,c] = occ + raw[x,y,c] *
+ * (1 - occ/denom), occ = sum of vessels[x0+x, y0+y, z] over zbounds[c] <=
+ * z < zbounds[c+1].  vessels: (vx,vy,vz) float32 device array; zbounds: HOST
+ * array of nz+1 rising entries in 0..vz (nz <= 512). */
+int mm_vessel_combine(const float* vessels, int vx, int vy, int vz, int x0, int y0, const int* zbounds,
+                      float denom, float* raw, int nx, int ny, int nz, void* stream);
+
+/* ------------------------------------------------------------------------
  * Local-PSF overlap-add render (RANA compact-support operator), FP64.
  * One call renders the volume through one FullFieldPSF (one depth):
  *   out[r] += sum over node pairs (i,j) of tile convolution / correlation.

@@ -119,6 +119,11 @@ SIGNATURES = {
                                  c_void_p, c_void_p]),
     "mm_resample_images": (c_int, [c_void_p, c_int, c_int, c_int, c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_int,
                                    c_int, c_int, c_float, c_void_p, c_void_p]),
+    "mm_gp_spectrum": (c_int, [c_int, c_int, c_int, c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_void_p,
+                               c_void_p, c_void_p, c_void_p, c_void_p]),
+    "mm_gp_finish": (c_int, [c_void_p, c_int, c_int, c_int, c_float, c_float, c_float, c_void_p, c_void_p]),
+    "mm_vessel_combine": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_int, c_void_p, c_float, c_void_p, c_int,
+                                  c_int, c_int, c_void_p]),
     "mm_local_render_workspace_size": (c_size_t, [POINTER(LocalDesc)]),
     "mm_local_render": (c_int, [POINTER(LocalDesc), c_void_p, c_void_p, c_void_p, c_void_p, c_size_t, c_void_p]),
 }

@@ -6,7 +6,8 @@ Run in a container where the reference source tree is mounted read-only:
 
 It imports the reference package from that path (no bytecode is written),
 runs its CPU optical stage (``maomi.optics.propagate``, ``v4_interpolate``,
-``resize_xy``, ``translate_xy``, ``pupil``) and its local
+``resize_xy``, ``translate_xy``, ``pupil``), its scattering-field generator
+(``prepare_fields``, ``masked_3DGP_test``) and its local
 PSF operator (``maomi.rana.RanaOperator``) on seeded inputs, and stores inputs
 (where small) and outputs as ``*.npz`` next to this script.  Large inputs are
 regenerated from their seeds by ``maomi_b200.synthetic`` and stored only as a
@@ -230,16 +231,48 @@ def make_local_fft(torch):
     return res
 
 
-def main(ref_path):
+def make_fields(torch):
+    """The scattering-field generator: masked_3DGP_test on odd and even grids
+    (the noise is re-drawn by the tests from the recorded seed: real parts,
+    then imaginary parts) and prepare_fields with a vessel occupancy volume."""
+    from maomi import _optical_math as legacy
+    from maomi.optics import OpticalConfig, prepare_fields
+    res = {}
+    for tag, shape, ls, p_scale in (("odd", (15, 22, 7), [[2.0, 3.0, 0.8], [5.0, 1.5, 2.5]], 3.0),
+                                    ("even", (24, 16, 6), [[1.2, 1.2, 0.4]], 1.0)):
+        seed = 1234 + len(tag)
+        torch.manual_seed(seed)
+        l = torch.tensor(ls, dtype=torch.float32)
+        w = torch.tensor([0.7, 0.3][:len(ls)], dtype=torch.float32)
+        out = legacy.masked_3DGP_test(shape, l, p_scale, l_weights=w, device="cpu")
+        res.update({f"{tag}_shape": np.array(shape), f"{tag}_ls": np.array(ls, np.float32), f"{tag}_w": w.numpy(),
+                    f"{tag}_p": np.float64(p_scale), f"{tag}_seed": np.int64(seed), f"{tag}_out": out.numpy()})
+    cfg = OpticalConfig(volume_um=(16.0, 16.0, 10.0), depth_um=20.0, tail_um=10.0)
+    rng = np.random.default_rng(5)
+    vessels = (rng.random((72, 72, 45)) < 0.05).astype(np.float32)
+    raw = [a.numpy() for a in prepare_fields(cfg, vessels, scatter=True)]
+    res.update({f"vessel_raw{i}": a for i, a in enumerate(raw)})
+    res["vessels_seed"] = np.int64(5)
+    res.update({"cfg_" + k: v for k, v in _cfg_dict(cfg).items()})
+    return res
+
+
+MAKERS = (("numerics", make_numerics), ("local_fft", make_local_fft), ("stage_small", make_stage_small),
+          ("stage_reftest", make_stage_reftest), ("stage_bench_sites", make_stage_bench_sites),
+          ("fields", make_fields))
+
+
+def main(ref_path, only=None):
     torch = _import_reference(ref_path)
     torch.set_num_threads(8)
-    for name, fn in (("numerics", make_numerics), ("local_fft", make_local_fft),
-                     ("stage_small", make_stage_small), ("stage_reftest", make_stage_reftest),
-                     ("stage_bench_sites", make_stage_bench_sites)):
+    for name, fn in MAKERS:
+        if only and name not in only:
+            continue
         out = fn(torch)
         np.savez_compressed(HERE / f"{name}.npz", **out)
         print(name, sum(np.asarray(v).nbytes for v in out.values()) // 1024, "KiB raw")
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    # make_golden.py [reference path] [fixture names...]
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference", sys.argv[2:] or None)
