@@ -73,16 +73,53 @@ __global__ void gp_spectrum_plane_kernel(int nx, int ny, int nz, const float* __
   float2* out = spec + (size_t)x * plane;
   const float* rs = re + (size_t)sx * plane;
   const float* is = im + (size_t)sx * plane;
+  // (y, z) of o = threadIdx.x + i * blockDim.x, stepped without divisions
+  const int dy = blockDim.x / nz, dz = blockDim.x % nz;
+  int y = threadIdx.x / nz, z = threadIdx.x % nz;
   for (int o = threadIdx.x; o < plane; o += blockDim.x) {
-    const int y = o / nz, z = o % nz;
     float acc = 0.f;
     for (int k = 0; k < K; ++k) {
       const float k3 = kx[k] * ky[k * ny + y] * kz[k * nz + z];
       acc += __ldg(prod_l + k) * (k3 * k3) * __ldg(w2 + k);
     }
     const float s = sqrtf(acc);
-    const int j = ((y + ny / 2) % ny) * nz + (z + nz / 2) % nz;
+    int sy = y + ny / 2, sz = z + nz / 2;
+    sy -= sy >= ny ? ny : 0;
+    sz -= sz >= nz ? nz : 0;
+    const int j = sy * nz + sz;
     out[o] = make_float2(__ldg(rs + j) * s, __ldg(is + j) * s);
+    z += dz;
+    y += dy;
+    if (z >= nz) {
+      z -= nz;
+      ++y;
+    }
+  }
+}
+
+// Plane-per-block form of gp_finish_kernel (same values).
+__global__ void gp_finish_plane_kernel(const float2* __restrict__ yv, int nx, int ny, int nz, float scale, float first,
+                                       float last, float* __restrict__ out) {
+  const int x = blockIdx.x, sx = (x + nx / 2) % nx;
+  const int plane = ny * nz;
+  const float2* src = yv + (size_t)sx * plane;
+  float* dst = out + (size_t)x * plane;
+  const int dy = blockDim.x / nz, dz = blockDim.x % nz;
+  int y = threadIdx.x / nz, z = threadIdx.x % nz;
+  for (int o = threadIdx.x; o < plane; o += blockDim.x) {
+    int sy = y + ny / 2, sz = z + nz / 2;
+    sy -= sy >= ny ? ny : 0;
+    sz -= sz >= nz ? nz : 0;
+    float v = scale * src[sy * nz + sz].x;
+    if (z == 0) v *= first;
+    if (z == nz - 1) v *= last;
+    dst[o] = v;
+    z += dz;
+    y += dy;
+    if (z >= nz) {
+      z -= nz;
+      ++y;
+    }
   }
 }
 
@@ -155,8 +192,12 @@ extern "C" int mm_gp_finish(const void* y, int nx, int ny, int nz, float scale, 
   MM_CHECK_ARG(nx >= 1 && ny >= 1 && nz >= 1, "bad GP grid %d x %d x %d", nx, ny, nz);
   MM_CHECK_ARG(y && out, "NULL pointer");
   const long long total = (long long)nx * ny * nz;
-  mm::gp_finish_kernel<<<mm::grid_of(total), 256, 0, static_cast<cudaStream_t>(stream)>>>(
-      static_cast<const float2*>(y), nx, ny, nz, scale, first, last, out);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if ((long long)ny * nz < (1ll << 31))
+    mm::gp_finish_plane_kernel<<<nx, 256, 0, s>>>(static_cast<const float2*>(y), nx, ny, nz, scale, first, last, out);
+  else
+    mm::gp_finish_kernel<<<mm::grid_of(total), 256, 0, s>>>(static_cast<const float2*>(y), nx, ny, nz, scale, first,
+                                                            last, out);
   MM_CHECK_LAUNCH("GP finish");
   return MM_OK;
 }
