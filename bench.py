@@ -52,7 +52,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--schedule", default="persistent", choices=["persistent", "batched"])
-    ap.add_argument("--slots", type=int, default=64)
+    ap.add_argument("--slots", type=int, default=96)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sites", type=int, default=8)
     ap.add_argument("--sites", type=int, default=SITES, help="profile a subset of the lattice (not a bench line)")

@@ -90,7 +90,7 @@ def assemble_sharded(config, parts, count, group=None, *, points_um, z_positions
     return res
 
 
-def run_stage_sharded(config, raw_fields, points_um=None, *, group=None, device=None, precision="compensated", slots=64):
+def run_stage_sharded(config, raw_fields, points_um=None, *, group=None, device=None, precision="compensated", slots=96):
     """The optical stage of one tissue block on every rank of `group`, each
     rank propagating its band of sites on its own GPU."""
     import torch
