@@ -92,19 +92,6 @@ __device__ __forceinline__ bool decode(const Params& p, long long item, Item& it
   return it.site < p.nsites;
 }
 
-__device__ __forceinline__ float block_sum(float v, float* red) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  __syncthreads();
-  if (lane == 0) red[warp] = v;
-  __syncthreads();
-  float s = 0.f;
-  if (threadIdx.x == 0)
-    for (int w = 0; w < int(blockDim.x >> 5); ++w) s += red[w];
-  return s;  // valid in thread 0
-}
-
 // Which line of the item this thread works on, and its place in the line:
 // rows (axis 0) keep a line's threads in one warp; columns (axis 1) put 32
 // consecutive columns in a warp so every global access is a full segment.
