@@ -39,6 +39,12 @@ const char* mm_last_error(void);
 /* 1 if the current device is an sm_100 part the library was built for. */
 int mm_device_supported(void);
 
+/* sizeof of a descriptor struct of this header, by its type name
+   ("mm_stage_plan", ...; 0 for an unknown name): lets a binding check its
+   own record layout against the library's.  No counterpart in the
+   reference, whose kernels take no structs. */
+size_t mm_struct_size(const char* name);
+
 /* Kernels launched by this library since it was loaded (all threads). */
 unsigned long long mm_launch_count(void);
 
@@ -215,6 +221,13 @@ typedef struct {
                               this count leave at once, so work queued on other
                               streams (e.g. the v4 factorisation) runs there
                               while the sites propagate; 0 = use every SM         */
+  /* fault drill for the bounded dependency wait (leave both 0 in production):
+     hold_site = s + 1 makes site s's first item wait for a counter value that
+     is never published, and spin_limit (> 0) replaces the default bound of
+     that wait (persistent schedule); the call then returns MM_ERR_TIMEOUT
+     with every CTA exited                                                    */
+  int hold_site;
+  long long spin_limit;
 } mm_stage_plan;
 
 enum {

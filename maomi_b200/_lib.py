@@ -34,7 +34,8 @@ class StagePlan(Structure):
                 ("cut", c_int), ("focal_x0", c_int), ("focal_y0", c_int), ("focal_h", c_int), ("focal_w", c_int),
                 ("tail_weight", c_void_p * 2), ("focal", c_void_p), ("tail_image", c_void_p * 2),
                 ("tail_per_site", c_int), ("tail_profile", c_void_p * 2), ("offsets", c_void_p), ("nsites", c_int),
-                ("precision", c_int), ("reserve_sms", c_int)]
+                ("precision", c_int), ("reserve_sms", c_int), ("hold_site", c_int),
+                ("spin_limit", ctypes.c_longlong)]
 
 
 class ItemClass(Structure):
@@ -81,6 +82,7 @@ SIGNATURES = {
     "mm_last_error": (c_char_p, []),
     "mm_device_supported": (c_int, []),
     "mm_launch_count": (ctypes.c_ulonglong, []),
+    "mm_struct_size": (ctypes.c_size_t, [c_char_p]),
     "mm_gemm_bf16_tn": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, c_int, c_void_p, c_int, c_void_p]),
     "mm_surrogate_layout": (c_int, [c_void_p, c_int]),
     "mm_surrogate_constants": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),

@@ -194,8 +194,14 @@ class OpticalPlan:
         return _lib.MM_SCHEDULE_PERSISTENT if schedule == "persistent" else _lib.MM_SCHEDULE_BATCHED
 
     # ------------------------------------------------------------ propagation
-    def run_sites(self, offsets, *, tail_per_site, slots, schedule=None, check=True, events=None, reserve_sms=0):
-        """Propagate every site; returns device buffers (focal, tail images, profiles)."""
+    def run_sites(self, offsets, *, tail_per_site, slots, schedule=None, check=True, events=None, reserve_sms=0,
+                  fault_drill=None):
+        """Propagate every site; returns device buffers (focal, tail images, profiles).
+
+        ``fault_drill`` (tests only): ``{"hold_site": s + 1, "spin_limit": polls}``
+        makes site s's first item wait for a counter that is never published,
+        so the persistent launch's bounded wait runs out and the call raises
+        the timeout error."""
         import torch
         dev = self.device
         P = len(offsets)
@@ -233,6 +239,9 @@ class OpticalPlan:
         plan.nsites = P
         plan.precision = _lib.PRECISIONS[self.precision]
         plan.reserve_sms = int(reserve_sms)
+        if fault_drill:
+            plan.hold_site = int(fault_drill.get("hold_site", 0))
+            plan.spin_limit = int(fault_drill.get("spin_limit", 0))
         lib = _lib.load()
         wbytes = lib.mm_propagate_workspace_size(plan, slots, sched)
         work = torch.empty(wbytes + 256, dtype=torch.uint8, device=dev)

@@ -42,3 +42,16 @@ extern "C" int mm_device_supported(void) {
   if (cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, dev) != cudaSuccess) return 0;
   return major == 10 && minor == 0;
 }
+
+extern "C" size_t mm_struct_size(const char* name) {
+  if (!name) return 0;
+  const std::string n(name);
+  if (n == "mm_pupil_desc") return sizeof(mm_pupil_desc);
+  if (n == "mm_base_desc") return sizeof(mm_base_desc);
+  if (n == "mm_stage_desc") return sizeof(mm_stage_desc);
+  if (n == "mm_stage_plan") return sizeof(mm_stage_plan);
+  if (n == "mm_item_class") return sizeof(mm_item_class);
+  if (n == "mm_local_desc") return sizeof(mm_local_desc);
+  if (n == "mm_surrogate_desc") return sizeof(mm_surrogate_desc);
+  return 0;
+}

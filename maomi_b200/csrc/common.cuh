@@ -15,6 +15,10 @@ namespace mm {
 void set_error(const char* fmt, ...);
 int cuda_status(cudaError_t e, const char* what);
 void count_launch();
+// Sites in flight that mm_propagate_sites actually uses for `slots` asked:
+// at most the site count, and for the persistent schedule balanced so the
+// last wave is (nearly) full.  Defined in propagate.cu.
+int propagation_slots(int nsites, int slots, int schedule);
 
 #define MM_CHECK_ARG(cond, ...)                     \
   do {                                              \

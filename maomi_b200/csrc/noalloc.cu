@@ -14,7 +14,10 @@
 //    for 31 sites in flight (1 MiB each); calls needing more are rejected.
 //  * The first call on a device looks up the array's device address (with
 //    that device current) and caches it; make that first call before any
-//    stream capture begins.
+//    stream capture begins.  The cache assumes the device keeps one primary
+//    context for the life of the process (as CUDA runtime and PyTorch
+//    programs do); if the cached address no longer belongs to the current
+//    context (after cudaDeviceReset, say) it is looked up again.
 //  * Every call shares the array and it keeps the last call's contents; the
 //    propagation clears its queue counters and error flag itself and writes
 //    every field buffer before reading it.  Calls whose work overlaps on the
@@ -41,6 +44,16 @@ int noalloc_scratch(void** out) {
   MM_CHECK_CUDA(cudaGetDevice(&dev), "cudaGetDevice");
   MM_CHECK_ARG(dev >= 0 && dev < kMaxDevices, "device ordinal %d beyond %d", dev, kMaxDevices);
   std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (g_noalloc_addr[dev]) {
+    // A context torn down and recreated (cudaDeviceReset) reloads the module;
+    // an address that is no longer device memory of this context is stale.
+    cudaPointerAttributes attr{};
+    if (cudaPointerGetAttributes(&attr, g_noalloc_addr[dev]) != cudaSuccess || attr.type != cudaMemoryTypeDevice ||
+        attr.device != dev) {
+      (void)cudaGetLastError();
+      g_noalloc_addr[dev] = nullptr;
+    }
+  }
   if (!g_noalloc_addr[dev]) {
     void* p = nullptr;
     MM_CHECK_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch), "cudaGetSymbolAddress(no-alloc scratch)");
@@ -57,6 +70,10 @@ extern "C" int mm_propagate_sites_noalloc(const mm_stage_plan* plan, int schedul
   using namespace mm;
   MM_CHECK_ARG(plan != nullptr, "plan is NULL");
   MM_CHECK_ARG(slots >= 1, "slots must be >= 1 (got %d)", slots);
+  MM_CHECK_ARG(plan->nsites >= 1, "nsites must be >= 1 (got %d)", plan->nsites);
+  // size the request as mm_propagate_sites will run it: clamped to the site
+  // count and balanced over the waves
+  slots = propagation_slots(plan->nsites, slots, schedule);
   const size_t need = mm_propagate_workspace_size(plan, slots, schedule);
   if (need > kNoAllocScratchBytes) {
     const size_t one = mm_propagate_workspace_size(plan, 1, schedule);

@@ -60,6 +60,8 @@ struct Params {
   int b_stage, b_k, b_site0;
   int precision;  // MM_PRECISION_*: arithmetic of the radix-2 line transforms
   int reserve_sms;  // persistent CTAs starting on SM ids below this leave at once
+  int hold_site;    // fault drill: site + 1 whose first item waits for ever (0 = off)
+  long long spin_limit;  // bound of a dependency wait, in polls
 };
 
 constexpr long long kSpinLimit = 1ll << 24;  // ~ seconds with the backoff below
@@ -319,7 +321,8 @@ __global__ void __launch_bounds__(LINES * L::R2, L::kMinBlocks * 128 / (LINES * 
   // counter value that publishes the segment before item it
   auto needed = [&](const Item& it) {
     const StageP& st = p.st[it.stage];
-    return unsigned(it.wave * p.blocks_per_site + st.cum0 + (long long)it.k * st.nblocks);
+    const unsigned held = (p.hold_site == it.site + 1) ? 0x40000000u : 0u;
+    return unsigned(it.wave * p.blocks_per_site + st.cum0 + (long long)it.k * st.nblocks) + held;
   };
   // thread 0: wait (bounded) until the item's inputs are published
   auto wait_for = [&](const Item& it) {
@@ -327,7 +330,7 @@ __global__ void __launch_bounds__(LINES * L::R2, L::kMinBlocks * 128 / (LINES * 
     long long spins = 0;
     unsigned ns = 32;
     while (ld_acquire(p.counters + it.slot) < need) {
-      if (++spins > kSpinLimit || (ld_acquire(reinterpret_cast<unsigned*>(p.error)) & 1u) != 0u) {
+      if (++spins > p.spin_limit || (ld_acquire(reinterpret_cast<unsigned*>(p.error)) & 1u) != 0u) {
         atomicOr(p.error, 1);
         return 1;
       }
@@ -605,11 +608,27 @@ int build_params(const mm_stage_plan* plan, int slots, Params& p) {
   p.precision = plan->precision;
   MM_CHECK_ARG(plan->reserve_sms >= 0 && plan->reserve_sms <= 64, "reserve_sms %d outside 0..64", plan->reserve_sms);
   p.reserve_sms = plan->reserve_sms;
+  MM_CHECK_ARG(plan->hold_site >= 0 && plan->hold_site <= plan->nsites, "hold_site %d outside 0..%d",
+               plan->hold_site, plan->nsites);
+  MM_CHECK_ARG(plan->spin_limit >= 0, "spin_limit must be >= 0");
+  p.hold_site = plan->hold_site;
+  p.spin_limit = plan->spin_limit > 0 ? plan->spin_limit : kSpinLimit;
   p.blocks_per_site = cum;
   return MM_OK;
 }
 
 }  // namespace
+
+int propagation_slots(int nsites, int slots, int schedule) {
+  slots = std::min(slots, nsites);
+  if (schedule == MM_SCHEDULE_PERSISTENT && slots > 0) {
+    // Balance the sites over the slots so the last wave is (nearly) full.
+    const int waves = (nsites + slots - 1) / slots;
+    slots = (nsites + waves - 1) / waves;
+  }
+  return slots;
+}
+
 }  // namespace mm
 
 extern "C" size_t mm_propagate_workspace_size(const mm_stage_plan* plan, int slots, int schedule) {
@@ -624,12 +643,7 @@ extern "C" int mm_propagate_sites(const mm_stage_plan* plan, int schedule, int s
   Params p;
   if (int rc = build_params(plan, slots, p)) return rc;
   MM_CHECK_ARG(schedule == MM_SCHEDULE_PERSISTENT || schedule == MM_SCHEDULE_BATCHED, "unknown schedule %d", schedule);
-  slots = std::min(slots, plan->nsites);
-  if (schedule == MM_SCHEDULE_PERSISTENT) {
-    // Balance the sites over the slots so the last wave is (nearly) full.
-    const int waves = (plan->nsites + slots - 1) / slots;
-    slots = (plan->nsites + waves - 1) / waves;
-  }
+  slots = propagation_slots(plan->nsites, slots, schedule);
   p.slots = slots;
   Workspace w = carve(workspace, plan->n, plan->n2, slots);
   MM_CHECK_ARG(workspace != nullptr && workspace_bytes >= w.bytes,

@@ -266,7 +266,9 @@ def stage_to_host(config, dev, *, return_psf_3d=True, out=None):
     return stage_result(config, stage_copy_async(dev, return_psf_3d=return_psf_3d, out=out))
 
 
-_PINNED_POOLS = {}
+#: pinned host buffer sets not held by a running ``run_stages`` call, keyed
+#: by the shapes of the products they hold
+_PINNED_FREE = {}
 
 
 def _pinned_set(dev, return_psf_3d):
@@ -291,40 +293,55 @@ def run_stages(config, blocks, points_um=None, *, device="cuda", depth=2, return
     while block i's products are copied to the host on a copy stream, block
     i+1 is uploaded and computed.  Yields the host dictionaries in order.
 
-    ``reuse=True`` copies into a pool of ``depth + 1`` pinned buffer sets kept
-    between calls (no page-locked allocation per block): a yielded result's
-    arrays stay valid until ``depth`` further results have been yielded."""
+    ``reuse=True`` copies into ``2 * depth`` pinned buffer sets that this call
+    takes from a pool kept between calls (no page-locked allocation per
+    block).  Block k's products land in set k mod 2*depth, which the copy of
+    block k + 2*depth overwrites; that copy is enqueued only after result
+    k + depth has been yielded, so a yielded result's arrays stay valid until
+    ``depth`` further results have been yielded.  Calls running side by side
+    hold disjoint sets.  When a call ends its sets return to the pool, and
+    the arrays of its last results stay valid until another ``reuse=True``
+    call starts."""
     import collections
     import torch
     copy = torch.cuda.Stream(device=device)
     up = torch.cuda.Stream(device=device)
     main = torch.cuda.current_stream(device)
     pending = collections.deque()
+    held = {}
     count = 0
-    for raw in blocks:
-        # uploads run on their own stream, so block i+1's fields cross PCIe
-        # while block i still computes; the compute stream waits for them
-        with torch.cuda.stream(up):
-            fields = [a.to(device, non_blocking=True) if isinstance(a, torch.Tensor) else _lib.upload(a, device)
-                      for a in raw]
-        main.wait_stream(up)
-        for f in fields:
-            f.record_stream(main)
-        dev = stage_device(config, fields, points_um, device=device, **kwargs)
-        out = None
-        if reuse:
-            key = (str(device), tuple((k, tuple(v.shape)) for k, v in dev.items() if hasattr(v, "shape")),
-                   len(dev["profiles"]), bool(return_psf_3d), depth)
-            pool = _PINNED_POOLS.setdefault(key, [])
-            if len(pool) < depth + 1:
-                pool.append(_pinned_set(dev, return_psf_3d))
-            out = pool[count % (depth + 1)]
-        pending.append(stage_copy_async(dev, return_psf_3d=return_psf_3d, out=out, stream=copy))
-        count += 1
-        if len(pending) >= depth:
+    try:
+        for raw in blocks:
+            # uploads run on their own stream, so block i+1's fields cross PCIe
+            # while block i still computes; the compute stream waits for them
+            with torch.cuda.stream(up):
+                fields = [a.to(device, non_blocking=True) if isinstance(a, torch.Tensor) else _lib.upload(a, device)
+                          for a in raw]
+            main.wait_stream(up)
+            for f in fields:
+                f.record_stream(main)
+            dev = stage_device(config, fields, points_um, device=device, **kwargs)
+            out = None
+            if reuse:
+                key = (str(device), tuple((k, tuple(v.shape)) for k, v in dev.items() if hasattr(v, "shape")),
+                       len(dev["profiles"]), bool(return_psf_3d))
+                sets = held.setdefault(key, [])
+                if len(sets) < 2 * depth:
+                    free = _PINNED_FREE.setdefault(key, [])
+                    sets.append(free.pop() if free else _pinned_set(dev, return_psf_3d))
+                out = sets[count % (2 * depth)]
+            pending.append(stage_copy_async(dev, return_psf_3d=return_psf_3d, out=out, stream=copy))
+            count += 1
+            if len(pending) >= depth:
+                yield stage_result(config, pending.popleft())
+        while pending:
             yield stage_result(config, pending.popleft())
-    while pending:
-        yield stage_result(config, pending.popleft())
+    finally:
+        # copies still in flight (a generator closed early) finish before
+        # their buffers can be handed to another call
+        copy.synchronize()
+        for key, sets in held.items():
+            _PINNED_FREE.setdefault(key, []).extend(sets)
 
 
 def run_stage(config, raw_fields, points_um=None, *, uin=None, device="cuda", tails=True, count_per_axis=65,

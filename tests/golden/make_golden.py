@@ -2,7 +2,7 @@
 
 Run in a container where the reference source tree is mounted read-only:
 
-    python tests/golden/make_golden.py /root/reference
+    python tests/golden/make_golden.py <path to the MaoMi source tree>
 
 It imports the reference package from that path (no bytecode is written),
 runs its CPU optical stage (``maomi.optics.propagate``, ``v4_interpolate``,
@@ -23,6 +23,9 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 REPO = HERE.parents[1]
+sys.path.insert(0, str(HERE))
+from lattice import (LATTICE_FULL_SITES, LATTICE_RAW_SEED, SKETCH_DIM, SKETCH_SEED,  # noqa: E402
+                     lattice_points, mask_pixels, psf_sketch)
 
 
 def _import_reference(path):
@@ -147,6 +150,64 @@ def make_stage_bench_sites(torch):
     return res
 
 
+def _lattice_result(prefix, out, full_psf):
+    ij = mask_pixels(np.shape(out["mask_raw"]))
+    flat = {f"{prefix}energies": np.asarray(out["energies"]),
+            f"{prefix}psf_sketch": psf_sketch(out["psf_3d"]),
+            f"{prefix}psf_site_norm": np.linalg.norm(np.asarray(out["psf_3d"], np.float64).reshape(
+                len(out["energies"]), -1), axis=1),
+            f"{prefix}psf": np.asarray(out["psf"], np.float32),
+            f"{prefix}psf_raw": np.asarray(out["psf_raw"], np.float32),
+            f"{prefix}mask_raw_px": out["mask_raw"][ij[:, 0], ij[:, 1]],
+            f"{prefix}mask_px": out["mask"][ij[:, 0], ij[:, 1]],
+            f"{prefix}mask_mean": np.asarray(out["mask_mean"]),
+            f"{prefix}negative_resampling_mass_fraction": np.asarray(out["negative_resampling_mass_fraction"])}
+    if full_psf:
+        flat[f"{prefix}psf_3d_sites"] = np.asarray(out["psf_3d"][LATTICE_FULL_SITES], np.float32)
+    for t in ("psfT", "psfB"):
+        tail = out[t]
+        flat[f"{prefix}{t}_convmask"] = np.asarray(tail["convmask"], np.float32)
+        flat[f"{prefix}{t}_weight"] = np.asarray(tail["weight"])
+        flat[f"{prefix}{t}_psfZ"] = np.asarray(tail["psfZ"])
+        flat[f"{prefix}{t}_mask_raw_px"] = tail["mask_raw"][ij[:, 0], ij[:, 1]]
+        flat[f"{prefix}{t}_mask_px"] = tail["mask"][ij[:, 0], ij[:, 1]]
+        flat[f"{prefix}{t}_mask_mean"] = np.asarray(tail["mask_mean"])
+    return flat
+
+
+def make_stage_bench_lattice(torch):
+    """Benchmark geometry (n=256, 60 screens, Zernike pupil, scattering
+    screens sigma=3 vox / RMS 0.015) on a 7 x 7 sub-lattice of the 65 x 65
+    site lattice: every product of ``maomi.optics.propagate`` in FP64 and
+    FP32.  psf_3d is stored in full for six sites and as a per-site sketch for
+    all 49; the 512 x 512 masks at 4,096 seeded pixels plus their means
+    (FP64 values rounded to float32 where marked)."""
+    from maomi.optics import OpticalConfig, pupil, propagate
+    from maomi.fixed import field_shapes, fixed_locations
+    from maomi_b200 import synthetic
+    cfg = synthetic.benchmark_stage_config(OpticalConfig)
+    raw = synthetic.raw_fields(cfg, field_shapes(cfg), sigma=3.0, rms=0.015, seed=LATTICE_RAW_SEED)
+    pts = lattice_points(fixed_locations, cfg)
+    res = {}
+    out = propagate(cfg, raw, pts, uin=pupil(cfg), device="cpu")
+    res.update(_lattice_result("f32_", out, full_psf=False))
+    old = torch.get_default_dtype()
+    torch.set_default_dtype(torch.float64)
+    try:
+        u64 = pupil(cfg)
+        out = propagate(cfg, [np.asarray(a, np.float64) for a in raw], pts, uin=u64.to(torch.complex128),
+                        device="cpu")
+        res.update(_lattice_result("f64_", out, full_psf=True))
+    finally:
+        torch.set_default_dtype(old)
+    res.update(points=pts, full_sites=LATTICE_FULL_SITES, mask_pixels=mask_pixels(out["mask_raw"].shape),
+               sketch_dim=np.asarray(SKETCH_DIM), sketch_seed=np.asarray(SKETCH_SEED),
+               raw_seed=np.asarray(LATTICE_RAW_SEED), raw_sigma=np.asarray(3.0), raw_rms=np.asarray(0.015),
+               raw_checksum=np.asarray([float(np.sum(a, dtype=np.float64)) for a in raw]))
+    res.update({"cfg_" + k: v for k, v in _cfg_dict(cfg).items()})
+    return res
+
+
 def make_numerics(torch):
     from maomi.numerics import resize_xy, translate_xy, v4_interpolate
     from maomi._propagation import edge_apodization
@@ -259,7 +320,7 @@ def make_fields(torch):
 
 MAKERS = (("numerics", make_numerics), ("local_fft", make_local_fft), ("stage_small", make_stage_small),
           ("stage_reftest", make_stage_reftest), ("stage_bench_sites", make_stage_bench_sites),
-          ("fields", make_fields))
+          ("fields", make_fields), ("stage_bench_lattice", make_stage_bench_lattice))
 
 
 def main(ref_path, only=None):
@@ -274,5 +335,7 @@ def main(ref_path, only=None):
 
 
 if __name__ == "__main__":
-    # make_golden.py [reference path] [fixture names...]
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference", sys.argv[2:] or None)
+    # make_golden.py <reference source tree> [fixture names...]
+    if len(sys.argv) < 2:
+        sys.exit("usage: make_golden.py <path to the MaoMi source tree> [fixture names...]")
+    main(sys.argv[1], sys.argv[2:] or None)

@@ -285,3 +285,53 @@ def test_single_site_stage_matches_oracle_fp64(small):
     assert np.allclose(out["mask_raw"], out["mask_raw"].flat[0])
     for t in ("psfT", "psfB"):
         assert rel_l2(out[t]["convmask"], ref[t]["convmask"]) < TOL
+
+
+@pytest.mark.gpu
+def test_reused_pinned_buffers_hold_for_depth_results(small):
+    """run_stages(reuse=True) over 5 blocks of 3 different tissues: every
+    result equals run_stage's, and each stays intact while ``depth`` further
+    results are yielded; a second generator running side by side never
+    writes into the first one's buffers."""
+    from maomi_b200 import synthetic
+    from maomi_b200.fixed import run_stage, run_stages
+    from oracle import optics as O
+    d, cfg, raw = small
+    tissues = [raw] + [synthetic.raw_fields(cfg, O.field_shapes(cfg), sigma=2.0, rms=0.01, seed=s) for s in (51, 52)]
+    expect = [run_stage(cfg, t, d["points"], precision="fp64")["psf_3d"] for t in tissues]
+    order = [0, 1, 2, 0, 1]
+    depth = 2
+    gen_a = run_stages(cfg, [tissues[i] for i in order], d["points"], precision="fp64", reuse=True, depth=depth)
+    gen_b = run_stages(cfg, [tissues[i] for i in reversed(order)], d["points"], precision="fp64", reuse=True,
+                       depth=depth)
+    got_a, got_b = [], []
+    for k in range(len(order)):
+        got_a.append(next(gen_a))
+        got_b.append(next(gen_b))
+        for j in range(max(0, k - depth), k + 1):
+            np.testing.assert_array_equal(got_a[j]["psf_3d"], expect[order[j]], err_msg=f"a: result {j} at {k}")
+            np.testing.assert_array_equal(got_b[j]["psf_3d"], expect[order[::-1][j]], err_msg=f"b: result {j} at {k}")
+    for g in (gen_a, gen_b):
+        with pytest.raises(StopIteration):
+            next(g)
+
+
+@pytest.mark.gpu
+def test_dependency_wait_runs_out_with_timeout_status(small):
+    """The persistent launch's bounded dependency wait: one site's first item
+    waits for a counter nothing publishes (a short poll limit), the kernel
+    sets its error flag, every CTA leaves, and the call reports the timeout.
+    The context stays usable: the next run matches a fresh plan's."""
+    import torch
+    from maomi_b200.backends.cuda.batched import OpticalPlan
+    d, cfg, raw = small
+    plan = OpticalPlan(cfg, raw)
+    _, off = plan.offsets(d["points"])
+    with torch.inference_mode():
+        with pytest.raises(RuntimeError, match="timed out"):
+            plan.run_sites(off, tail_per_site=True, slots=4, schedule="persistent",
+                           fault_drill={"hold_site": 3, "spin_limit": 2048})
+        torch.cuda.synchronize()
+        again = plan.run_sites(off, tail_per_site=True, slots=4, schedule="persistent")["focal"].cpu().numpy()
+        fresh = OpticalPlan(cfg, raw).run_sites(off, tail_per_site=True, slots=4)["focal"].cpu().numpy()
+    np.testing.assert_array_equal(again, fresh)

@@ -141,6 +141,19 @@ def test_header_symbols_exported():
     assert lib.mm_version() >= 100
 
 
+def test_descriptor_layouts_match_the_library():
+    """The ctypes records bind the C structs byte for byte (sizes agree)."""
+    import ctypes
+    from maomi_b200 import _lib
+    lib = _lib.load()
+    for name, cls in (("mm_stage_desc", _lib.StageDesc), ("mm_stage_plan", _lib.StagePlan),
+                      ("mm_item_class", _lib.ItemClass), ("mm_pupil_desc", _lib.PupilDesc),
+                      ("mm_base_desc", _lib.BaseDesc), ("mm_local_desc", _lib.LocalDesc),
+                      ("mm_surrogate_desc", _lib.SurrogateDesc)):
+        assert lib.mm_struct_size(name.encode()) == ctypes.sizeof(cls), name
+    assert lib.mm_struct_size(b"nothing") == 0
+
+
 def test_status_mapping():
     from maomi_b200 import _lib
     _lib.check(0)

@@ -85,19 +85,38 @@ def test_noalloc_matches_workspace_entry_point(schedule):
             assert rel_l2(a, b) <= TOL, (call, key, rel_l2(a, b))
 
 
-def test_noalloc_rejects_oversized_plans():
-    from oracle import optics as O
-    from maomi_b200 import _lib, synthetic
-    from maomi_b200.backends.cuda.batched import OpticalPlan
+def _small_plan(count_per_axis):
     import torch
+    from oracle import optics as O
+    from maomi_b200 import synthetic
+    from maomi_b200.backends.cuda.batched import OpticalPlan
+    from maomi_b200.fixed import fixed_locations
     d = golden("stage_small")
     cfg = cfg_from(d)
     raw = synthetic.raw_fields(cfg, O.field_shapes(cfg), sigma=float(d["raw_sigma"]), rms=float(d["raw_rms"]),
                                seed=int(d["raw_seed"]))
     plan = OpticalPlan(cfg, raw)
-    _, off_np = plan.offsets(d["points"])
-    off = torch.as_tensor(off_np, device="cuda")
+    _, off_np = plan.offsets(fixed_locations(cfg, count_per_axis))
+    return plan, torch.as_tensor(off_np, device="cuda")
+
+
+def test_noalloc_sizes_requests_as_they_run():
+    """A request is sized after the same clamping the workspace entry point
+    applies (at most one slot per site, waves balanced): 4,096 slots asked
+    for the 9-site plan run as 9 and fit; 144 sites in flight at 128 x 128
+    (256 KiB each, 36 MiB) do not fit the 32 MiB array and are rejected."""
+    from maomi_b200 import _lib
+    lib = _lib.load()
+    stream = _lib.stream_of("cuda")
+    plan, off = _small_plan(3)
     outs = _outputs(plan, off.shape[0])
-    rc = _lib.load().mm_propagate_sites_noalloc(_plan_struct(plan, off, outs), 0, 4096, 1, _lib.stream_of("cuda"))
-    assert rc == _lib.MM_ERR_ARGUMENT
-    assert "static array" in _lib.last_error()
+    _lib.check(lib.mm_propagate_sites_noalloc(_plan_struct(plan, off, outs), 0, 4096, 1, stream))
+    assert np.isfinite(outs["focal"].cpu().numpy()).all()
+    plan, off = _small_plan(12)
+    outs = _outputs(plan, off.shape[0])
+    for slots in (144, 4096):
+        rc = lib.mm_propagate_sites_noalloc(_plan_struct(plan, off, outs), 0, slots, 1, stream)
+        assert rc == _lib.MM_ERR_ARGUMENT
+        assert "static array" in _lib.last_error()
+    # 72 slots balance to 72 (two waves of 72): 18 MiB, accepted
+    _lib.check(lib.mm_propagate_sites_noalloc(_plan_struct(plan, off, outs), 0, 72, 1, stream))
