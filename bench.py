@@ -560,7 +560,9 @@ def main():
           "reuse": True}
     if args.reserve_sms is not None:
         kw["reserve_sms"] = args.reserve_sms
-    for _ in run_stages(cfg, [raw_pinned] * 3, points, device=dev, **kw):
+    # warm-up: at least 2 * depth blocks, so every pinned buffer set the
+    # timed run cycles through exists before timing starts
+    for _ in run_stages(cfg, [raw_pinned] * max(4, args.warmup), points, device=dev, **kw):
         pass
     h2d = sum(a.numel() * a.element_size() for a in raw_pinned)
     e_start, e_stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
