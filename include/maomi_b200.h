@@ -362,27 +362,50 @@ int mm_vessel_combine(const float* vessels, int vx, int vy, int vz, int x0, int 
 
 /* ------------------------------------------------------------------------
  * Local-PSF overlap-add render (RANA compact-support operator), FP64.
- * One call renders the volume through one FullFieldPSF (one depth):
- *   out[r] += sum over node pairs (i,j) of tile convolution / correlation.
+ * One call renders the volume through one FullFieldPSF, or through every
+ * field of a depth bank weighted per plane:
+ *   out[r] += sum over fields f and node pairs (i,j) of the pair's tile
+ *             correlation / convolution, weighted as the reference weights it.
  * Replaces LocalFFTPlan.__call__, maomi/rana/_fft.py:74-95 (with the plan
- * construction of :9-49 done on the host).
+ * construction of :9-49 done on the host by mm_local_tiles), and the
+ * per-field loop of RanaOperator.static, maomi/rana/operator.py:122-134.
  */
 typedef struct {
   int sx, sy, sz;          /* volume shape (X,Y,Z)                              */
   int kx, ky, kz;          /* kernel shape                                      */
   int nodes_x, nodes_y;    /* field nodes                                       */
-  const double* kernels;   /* (nodes_x, nodes_y, kx, ky, kz)                    */
+  const double* kernels;   /* (nfields, nodes_x, nodes_y, kx, ky, kz)           */
   const double* wx;        /* (nodes_x, sx) lateral weights                     */
   const double* wy;        /* (nodes_y, sy)                                     */
   int detection;           /* 1: weight sources before convolving              */
   int correlate;           /* 1: flipped kernel (excitation)                   */
   int plane;               /* 1: 2-D per-plane, output summed over z (scan_slab) */
+  int nfields;             /* depth fields in `kernels` (1 unless a bank)       */
+  const int32_t* tiles_x;  /* excitation/native: device copy of mm_local_tiles  */
+  int ntiles_x;            /*   of wx (ignored for detection)                   */
+  const int32_t* tiles_y;  /*   and of wy                                       */
+  int ntiles_y;
 } mm_local_desc;
 
+/* Host-side plan step (no device work): split the output pixels [0, n) of one
+ * axis into tiles over which the set of nodes with nonzero weight in
+ * w (nodes, n; HOST array) is constant and at most 4 nodes, each at most
+ * max_len (<= 18; 0 = 18) pixels long.  Writes up to `capacity` records of 8
+ * int32 {start, length, active count, node[4], 0} to `table` (may be NULL)
+ * and returns the number of tiles (n is always enough capacity), or a
+ * negative status.  Counterpart of the node-pair tiling of
+ * maomi/rana/_fft.py:24-49. */
+int mm_local_tiles(const double* w, int nodes, int n, int max_len, int32_t* table, int capacity);
+
+/* Bytes of device workspace mm_local_render needs (the source transposed). */
 size_t mm_local_render_workspace_size(const mm_local_desc* desc);
 
+/* zweight: (nfields, sz) device array or NULL (nfields == 1, weight 1):
+ * excitation/native weight output plane z, detection weights source plane z.
+ * Plane mode takes one field and no zweight (weight the source beforehand).
+ * `out` is accumulated into. */
 int mm_local_render(const mm_local_desc* desc, const double* source /* (sx,sy,sz) */,
-                    const double* zweight /* (sz) or NULL */, double* out /* (sx,sy[,sz]) */,
+                    const double* zweight, double* out /* (sx,sy[,sz]) */,
                     void* workspace, size_t workspace_bytes, void* stream);
 
 /* ------------------------------------------------------------------------

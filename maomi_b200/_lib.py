@@ -61,7 +61,8 @@ class BaseDesc(Structure):
 class LocalDesc(Structure):
     _fields_ = [("sx", c_int), ("sy", c_int), ("sz", c_int), ("kx", c_int), ("ky", c_int), ("kz", c_int),
                 ("nodes_x", c_int), ("nodes_y", c_int), ("kernels", c_void_p), ("wx", c_void_p), ("wy", c_void_p),
-                ("detection", c_int), ("correlate", c_int), ("plane", c_int)]
+                ("detection", c_int), ("correlate", c_int), ("plane", c_int), ("nfields", c_int),
+                ("tiles_x", c_void_p), ("ntiles_x", c_int), ("tiles_y", c_void_p), ("ntiles_y", c_int)]
 
 
 class SurrogateDesc(ctypes.Structure):
@@ -126,6 +127,7 @@ SIGNATURES = {
     "mm_gp_finish": (c_int, [c_void_p, c_int, c_int, c_int, c_float, c_float, c_float, c_void_p, c_void_p]),
     "mm_vessel_combine": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_int, c_void_p, c_float, c_void_p, c_int,
                                   c_int, c_int, c_void_p]),
+    "mm_local_tiles": (c_int, [c_void_p, c_int, c_int, c_int, c_void_p, c_int]),
     "mm_local_render_workspace_size": (c_size_t, [POINTER(LocalDesc)]),
     "mm_local_render": (c_int, [POINTER(LocalDesc), c_void_p, c_void_p, c_void_p, c_void_p, c_size_t, c_void_p]),
 }

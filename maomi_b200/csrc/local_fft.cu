@@ -2,49 +2,274 @@
 //
 // The reference evaluates, for every field-node pair (i, j), an FFT
 // convolution of the source tile around the node's support and overlap-adds
-// the weighted piece (maomi/rana/_fft.py:74-95).  Because every tile is zero
-// padded to a linear-convolution length, that equals the direct sum
+// the weighted piece (maomi/rana/_fft.py:74-95).  Every tile is zero padded to
+// a linear-convolution length, so that equals the direct sum
 //
 //   excitation (correlate): out[r] += wz(r_z) sum_ij w_ij(r) sum_u src[r + u - K/2]   k_ij[u]
 //   native (convolve)     : out[r] += wz(r_z) sum_ij w_ij(r) sum_u src[r - u + K/2]   k_ij[u]
 //   detection (convolve)  : out[r] +=         sum_ij sum_u w_ij(s) wz(s_z) src[s] k_ij[u],  s = r - u + K/2
 //
-// with zero source outside the volume (K/2 = floor per axis; plane mode sums
-// the 2-D operator over z with kernel plane z acting on source plane z).  This
-// kernel computes that sum directly in FP64: one CTA per output tile of
-// 16 x 16 pixels x 4 planes, looping over the node pairs active on the tile;
-// per kernel plane the four source planes (with halo) and the kernel plane are
-// staged in shared memory, and each thread slides an 8-wide register window
-// along y so every staged value feeds 8 FMAs.  Convolutions are turned into
-// correlations by staging the kernel flipped.
+// with w_ij(r) = wx[i, r_x] wy[j, r_y], zero source outside the volume
+// (K/2 = floor per axis) and, in plane mode, the 2-D operator summed over z
+// with kernel plane z acting on source plane z.  Convolutions become
+// correlations with the kernel staged flipped.
+//
+// Two kernels evaluate that sum in FP64:
+//
+// * cell_kernel (excitation, native): the output is cut along x and along y
+//   into tiles over which the set of nodes with nonzero weight is constant
+//   (mm_local_tiles; the smoothstep weights give two nodes per axis, so a tile
+//   of one node interval needs exactly its 2 x 2 node pairs, where a fixed
+//   16 x 16 grid straddling the intervals touched about nine).  One CTA owns a
+//   tile (<= 18 x 18 pixels) x 2 planes and loops over the depth fields whose
+//   weight is nonzero on its planes, so a whole depth bank is one launch.
+//   Per kernel plane it stages the source halo plane(s) and the four pairs'
+//   kernel planes in shared memory; each thread slides a register window of
+//   2 x 6 source values along y for 6 outputs and keeps one 6-wide
+//   accumulator per pair (24 FMAs per staged kernel value quartet), and folds
+//   the pairs with their pixel weights at the end.
+// * generic_kernel (detection, where the weights sit on the source side):
+//   16 x 16 x 4 output tiles, node pairs whose weighted source reaches the
+//   tile, source halo staged pre-weighted per pair.
+//
+// Both read the source transposed to (z, x, y) (a workspace filled by
+// transpose_kernel) so every staged halo row is a contiguous run of y.
 #include <algorithm>
+#include <vector>
 
 #include "common.cuh"
 
 namespace mm {
 namespace {
 
-constexpr int TX = 16, TY = 16, TZ = 4;  // output tile
-constexpr int QY = 8;                    // y outputs per thread (register window)
-constexpr int THREADS = TX * (TY / QY) * TZ;  // 128
+constexpr int kMaxNodes = 64;  // field nodes per axis
+constexpr int kTileInts = 8;   // mm_local_tiles record: start, len, nact, node[4], 0
+constexpr int kMaxActive = 4;  // nodes with nonzero weight inside one tile, per axis
 
-struct LocalP {
-  int sx, sy, sz, kx, ky, kz, nx, ny;
-  int kyp;         // ky padded to a multiple of QY
-  int hx, hy;      // staged halo extents: TX + kx - 1, TY + kyp - 1 (+QY slack)
-  const double* kern;
-  const double* wx;
-  const double* wy;
-  const double* wz;  // nullable
-  int detection, flip, plane;
-  int cx, cy, cz;  // correlation offsets of the staged (possibly flipped) kernel
+// ------------------------------------------------------------ common pieces
+__global__ void transpose_kernel(const double* __restrict__ src, int sx, int sy, int sz, double* __restrict__ dst) {
+  // src (x, y, z) -> dst (z, x, y); one CTA per (x, 32-row block of y)
+  __shared__ double t[32][17];
+  const int x = blockIdx.x;
+  const int y0 = blockIdx.y * 32;
+  for (int z0 = 0; z0 < sz; z0 += 16) {
+    for (int e = threadIdx.x; e < 32 * 16; e += blockDim.x) {
+      const int yy = e / 16, zz = e % 16;
+      const int y = y0 + yy, z = z0 + zz;
+      t[yy][zz] = (y < sy && z < sz) ? src[((size_t)x * sy + y) * sz + z] : 0.0;
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < 32 * 16; e += blockDim.x) {
+      const int zz = e / 32, yy = e % 32;
+      const int y = y0 + yy, z = z0 + zz;
+      if (y < sy && z < sz) dst[((size_t)z * sx + x) * sy + y] = t[yy][zz];
+    }
+    __syncthreads();
+  }
+}
+
+struct Common {
+  int sx, sy, sz, kx, ky, kz, nx, ny, nf;
+  const double* kern;   // (nf, nx, ny, kx, ky, kz)
+  const double* wx;     // (nx, sx)
+  const double* wy;     // (ny, sy)
+  const double* wz;     // (nf, sz) or null
+  const double* srcT;   // (sz, sx, sy)
   double* out;
-  const double* src;
+  int flip, plane;
+  int cx, cy, cz;       // correlation offsets of the staged (possibly flipped) kernel
 };
 
-__device__ __forceinline__ double wz_at(const LocalP& p, int z) { return p.wz ? p.wz[z] : 1.0; }
+__device__ __forceinline__ double wz_at(const Common& c, int f, int z) { return c.wz ? c.wz[(size_t)f * c.sz + z] : 1.0; }
 
-constexpr int kMaxNodes = 64;  // field nodes per axis
+__device__ __forceinline__ double kernel_tap(const Common& c, const double* kij, int ux, int uy, int kp) {
+  const int fx = c.flip ? c.kx - 1 - ux : ux, fy = c.flip ? c.ky - 1 - uy : uy;
+  return kij[((size_t)fx * c.ky + fy) * c.kz + kp];
+}
+
+// ---------------------------------------------------- cell kernel (gather)
+constexpr int QY = 6;              // y outputs per thread
+constexpr int TMAX = 18;           // tile extent per axis
+constexpr int CH = TMAX / QY;      // y chunks per tile row
+constexpr int GROUP = 64;          // threads per output plane (>= TMAX * CH)
+constexpr int TZC = 2;             // output planes per CTA
+constexpr int CELL_THREADS = GROUP * TZC;
+constexpr int PG = 4;              // node pairs per register pass
+static_assert(TMAX * CH <= GROUP, "one unit per thread");
+
+struct CellP {
+  Common c;
+  const int* tx;   // x tiles (kTileInts each)
+  const int* ty;
+  int ntx, nty;
+  int hx, hy;      // halo plane extents (hy padded against bank conflicts)
+  int kplanes;     // kernel-plane slots in shared memory (1, or TZC in plane mode)
+};
+
+__global__ void __launch_bounds__(CELL_THREADS, 2) cell_kernel(CellP P) {
+  extern __shared__ double smem[];
+  const Common& c = P.c;
+  const int* tx = P.tx + (size_t)(blockIdx.x / P.nty) * kTileInts;
+  const int* ty = P.ty + (size_t)(blockIdx.x % P.nty) * kTileInts;
+  const int x0 = tx[0], lx = tx[1], ax = tx[2];
+  const int y0 = ty[0], ly = ty[1], ay = ty[2];
+  // a malformed tile record renders nothing rather than reading out of bounds
+  bool ok = lx >= 1 && lx <= TMAX && ly >= 1 && ly <= TMAX && ax >= 1 && ax <= kMaxActive && ay >= 1 &&
+            ay <= kMaxActive && x0 >= 0 && x0 + lx <= c.sx && y0 >= 0 && y0 + ly <= c.sy;
+  for (int m = 0; m < kMaxActive; ++m) {
+    ok = ok && (m >= ax || (tx[3 + m] >= 0 && tx[3 + m] < c.nx));
+    ok = ok && (m >= ay || (ty[3 + m] >= 0 && ty[3 + m] < c.ny));
+  }
+  if (!ok) return;  // uniform per CTA
+  const int tid = threadIdx.x;
+  const int g = tid / GROUP;                 // plane group
+  const int u = tid % GROUP;
+  const int ch = u / TMAX, row = u % TMAX;   // rows fastest: conflict-free halo reads
+  const bool unit = u < TMAX * CH && row < lx && ch * QY < ly;
+  const int z0 = c.plane ? 0 : blockIdx.y * TZC;
+  const int oz = z0 + g;                     // 3-D: this group's output plane
+  const int hplane = P.hx * P.hy;
+  const int kplane = c.kx * c.ky;
+  double* halo = smem;                                         // [TZC][hx][hy]
+  double* ks = smem + (size_t)TZC * hplane;                    // [kplanes][PG][kx][ky]
+  const int npairs = ax * ay;
+  const int iters = c.plane ? (c.kz + TZC - 1) / TZC : c.kz;
+
+  double fin[QY];
+#pragma unroll
+  for (int q = 0; q < QY; ++q) fin[q] = 0.0;
+
+  for (int f = 0; f < c.nf; ++f) {
+    // skip fields with zero weight on this CTA's planes (uniform per CTA)
+    if (!c.plane && c.wz) {
+      bool any = false;
+      for (int zz = z0; zz < min(z0 + TZC, c.sz); ++zz) any |= (c.wz[(size_t)f * c.sz + zz] != 0.0);
+      if (!any) continue;
+    }
+    const double wzo = (!c.plane && oz < c.sz) ? wz_at(c, f, oz) : 1.0;
+    const bool live = unit && (c.plane || (oz < c.sz && wzo != 0.0));
+    const double* kf = c.kern + (size_t)f * c.nx * c.ny * kplane * c.kz;
+    for (int p0 = 0; p0 < npairs; p0 += PG) {
+      const int np = min(PG, npairs - p0);
+      double acc[PG][QY];
+#pragma unroll
+      for (int p = 0; p < PG; ++p)
+#pragma unroll
+        for (int q = 0; q < QY; ++q) acc[p][q] = 0.0;
+      for (int it = 0; it < iters; ++it) {
+        __syncthreads();
+        // ---- source halo: plane for each group (zero outside the volume)
+        for (int e = tid; e < TZC * hplane; e += CELL_THREADS) {
+          const int gg = e / hplane, rem = e % hplane, hxi = rem / P.hy, hyi = rem % P.hy;
+          int gz;
+          if (c.plane) gz = it * TZC + gg;
+          else gz = z0 + gg + it - c.cz;
+          const int gx = x0 - c.cx + hxi, gy = y0 - c.cy + hyi;
+          double v = 0.0;
+          if (gx >= 0 && gx < c.sx && gy >= 0 && gy < c.sy && gz >= 0 && gz < c.sz && (c.plane ? gz < c.kz : true))
+            v = c.srcT[((size_t)gz * c.sx + gx) * c.sy + gy];
+          halo[e] = v;
+        }
+        // ---- kernel planes of this pass's pairs (flipped for convolutions)
+        for (int e = tid; e < P.kplanes * np * kplane; e += CELL_THREADS) {
+          const int slot = e / (np * kplane), rem = e % (np * kplane), p = rem / kplane, uv = rem % kplane;
+          const int ux = uv / c.ky, uy = uv % c.ky;
+          const int pair = p0 + p, i = tx[3 + pair / ay], j = ty[3 + pair % ay];
+          const double* kij = kf + ((size_t)i * c.ny + j) * kplane * c.kz;
+          int kp;
+          if (c.plane) kp = it * TZC + slot;
+          else kp = c.flip ? c.kz - 1 - it : it;
+          ks[((size_t)slot * PG + p) * kplane + uv] = kp < c.kz ? kernel_tap(c, kij, ux, uy, kp) : 0.0;
+        }
+        __syncthreads();
+        if (!live) continue;
+        if (c.plane && it * TZC + g >= c.kz) continue;
+        const double* hbase = halo + (size_t)g * hplane + (size_t)row * P.hy + ch * QY;
+        const double* kbase = ks + (size_t)(c.plane ? g : 0) * PG * kplane;
+        for (int ux = 0; ux < c.kx; ++ux) {
+          const double* hrow = hbase + (size_t)ux * P.hy;
+          const double* krow = kbase + (size_t)ux * c.ky;
+          double w[2 * QY];
+#pragma unroll
+          for (int q = 0; q < QY; ++q) w[q] = hrow[q];
+          for (int uy0 = 0; uy0 < c.ky; uy0 += QY) {
+#pragma unroll
+            for (int q = 0; q < QY; ++q) w[QY + q] = hrow[uy0 + QY + q];
+            const int nph = min(QY, c.ky - uy0);
+#pragma unroll
+            for (int ph = 0; ph < QY; ++ph) {
+              if (ph < nph) {
+#pragma unroll
+                for (int p = 0; p < PG; ++p) {
+                  if (p < np) {
+                    const double kv = krow[(size_t)p * kplane + uy0 + ph];
+#pragma unroll
+                    for (int q = 0; q < QY; ++q) acc[p][q] = fma(w[q + ph], kv, acc[p][q]);
+                  }
+                }
+              }
+            }
+#pragma unroll
+            for (int q = 0; q < QY; ++q) w[q] = w[QY + q];
+          }
+        }
+      }
+      // ---- fold the pairs with their pixel weights
+      if (live) {
+        const int ox = x0 + row;
+#pragma unroll
+        for (int p = 0; p < PG; ++p) {
+          if (p < np) {
+            const int pair = p0 + p, i = tx[3 + pair / ay], j = ty[3 + pair % ay];
+            const double wxi = c.wx[(size_t)i * c.sx + ox] * wzo;
+#pragma unroll
+            for (int q = 0; q < QY; ++q) {
+              const int oy = y0 + ch * QY + q;
+              const double wyj = oy < c.sy ? c.wy[(size_t)j * c.sy + oy] : 0.0;
+              fin[q] = fma(wxi * wyj, acc[p][q], fin[q]);
+            }
+          }
+        }
+      }
+    }
+  }
+  // ---- write: 3-D, one writer per voxel; plane mode, the groups' partial
+  // sums over kernel planes are reduced through shared memory first
+  if (c.plane) {
+    __syncthreads();
+    double* red = smem;
+    if (g > 0 && unit)
+#pragma unroll
+      for (int q = 0; q < QY; ++q) red[((size_t)(g - 1) * GROUP + u) * QY + q] = fin[q];
+    __syncthreads();
+    if (g != 0 || !unit) return;
+    for (int gg = 1; gg < TZC; ++gg)
+#pragma unroll
+      for (int q = 0; q < QY; ++q) fin[q] += red[((size_t)(gg - 1) * GROUP + u) * QY + q];
+  }
+  if (!unit || (!c.plane && oz >= c.sz)) return;
+  const int ox = x0 + row;
+#pragma unroll
+  for (int q = 0; q < QY; ++q) {
+    const int yq = ch * QY + q;
+    if (yq >= ly) continue;
+    const int oy = y0 + yq;
+    double* dst = c.plane ? c.out + (size_t)ox * c.sy + oy : c.out + ((size_t)ox * c.sy + oy) * c.sz + oz;
+    *dst += fin[q];
+  }
+}
+
+// ------------------------------------------------- generic kernel (detection)
+constexpr int TX = 16, TY = 16, TZ = 4;  // output tile
+constexpr int GQY = 8;                   // y outputs per thread (register window)
+constexpr int GEN_THREADS = TX * (TY / GQY) * TZ;  // 128
+
+struct GenP {
+  Common c;
+  int kyp;         // ky padded to a multiple of GQY
+  int hx, hy;
+  int detection;
+};
 
 // Support [lo, hi] (first / last nonzero sample) of every node's weight row.
 __device__ void node_support(const double* w, int nodes, int n, int* lo, int* hi) {
@@ -61,157 +286,269 @@ __device__ void node_support(const double* w, int nodes, int n, int* lo, int* hi
   __syncthreads();
 }
 
-// Node with support [lo, hi] touches [a, b)?
 __device__ __forceinline__ bool touches(int lo, int hi, int a, int b) { return lo <= hi && lo < b && hi >= a; }
 
-__global__ void __launch_bounds__(THREADS) local_render_kernel(LocalP p) {
+__global__ void __launch_bounds__(GEN_THREADS) generic_kernel(GenP P) {
   extern __shared__ double smem[];
-  const int tiles_y = (p.sy + TY - 1) / TY;
+  const Common& c = P.c;
+  const int tiles_y = (c.sy + TY - 1) / TY;
   const int x0 = (blockIdx.x / tiles_y) * TX;
   const int y0 = (blockIdx.x % tiles_y) * TY;
-  const int z0 = p.plane ? 0 : blockIdx.y * TZ;
-  const int nzo = p.plane ? 1 : TZ;   // output planes of this tile
+  const int z0 = c.plane ? 0 : blockIdx.y * TZ;
+  const int nzo = c.plane ? 1 : TZ;
   const int tid = threadIdx.x;
-  const int tx = tid % TX, tq = (tid / TX) % (TY / QY), tzi = tid / (TX * (TY / QY));
+  const int tx = tid % TX, tq = (tid / TX) % (TY / GQY), tzi = tid / (TX * (TY / GQY));
   __shared__ int lox[kMaxNodes], hix[kMaxNodes], loy[kMaxNodes], hiy[kMaxNodes];
-  node_support(p.wx, p.nx, p.sx, lox, hix);
-  node_support(p.wy, p.ny, p.sy, loy, hiy);
-  const int hplane = p.hx * p.hy;
+  node_support(c.wx, c.nx, c.sx, lox, hix);
+  node_support(c.wy, c.ny, c.sy, loy, hiy);
+  const int hplane = P.hx * P.hy;
   double* halo = smem;                       // [TZ][hx][hy]
   double* ks = smem + (size_t)TZ * hplane;   // [kx][kyp]
-  // Source reach of the tile along x / y (for the node-activity test in detection mode).
-  const int sx_lo = x0 - p.cx, sx_hi = x0 + TX - 1 - p.cx + p.kx;
-  const int sy_lo = y0 - p.cy, sy_hi = y0 + TY - 1 - p.cy + p.kyp;
-  double acc_total[QY];
+  const int sx_lo = x0 - c.cx, sx_hi = x0 + TX - 1 - c.cx + c.kx;
+  const int sy_lo = y0 - c.cy, sy_hi = y0 + TY - 1 - c.cy + P.kyp;
+  // source planes this tile reaches (detection weights sit on the source)
+  const int szlo = c.plane ? 0 : max(0, z0 - c.cz), szhi = c.plane ? c.sz - 1 : min(c.sz - 1, z0 + TZ - 1 + c.kz - 1 - c.cz);
+  double acc_total[GQY];
 #pragma unroll
-  for (int q = 0; q < QY; ++q) acc_total[q] = 0.0;
-  for (int i = 0; i < p.nx; ++i) {
-    const bool ai = p.detection ? touches(lox[i], hix[i], sx_lo, sx_hi) : touches(lox[i], hix[i], x0, x0 + TX);
-    if (!ai) continue;
-    for (int j = 0; j < p.ny; ++j) {
-      const bool aj = p.detection ? touches(loy[j], hiy[j], sy_lo, sy_hi) : touches(loy[j], hiy[j], y0, y0 + TY);
-      if (!aj) continue;
-      const double* kij = p.kern + ((size_t)i * p.ny + j) * p.kx * p.ky * p.kz;
-      double acc[QY];
+  for (int q = 0; q < GQY; ++q) acc_total[q] = 0.0;
+  for (int f = 0; f < c.nf; ++f) {
+    if (c.wz) {
+      bool any = false;
+      if (P.detection) {
+        for (int zz = szlo; zz <= szhi; ++zz) any |= wz_at(c, f, zz) != 0.0;
+      } else {
+        for (int zz = z0; zz < min(z0 + nzo, c.sz); ++zz) any |= wz_at(c, f, zz) != 0.0;
+      }
+      if (!any) continue;
+    }
+    const double* kf = c.kern + (size_t)f * c.nx * c.ny * c.kx * c.ky * c.kz;
+    for (int i = 0; i < c.nx; ++i) {
+      const bool ai = P.detection ? touches(lox[i], hix[i], sx_lo, sx_hi) : touches(lox[i], hix[i], x0, x0 + TX);
+      if (!ai) continue;
+      for (int j = 0; j < c.ny; ++j) {
+        const bool aj = P.detection ? touches(loy[j], hiy[j], sy_lo, sy_hi) : touches(loy[j], hiy[j], y0, y0 + TY);
+        if (!aj) continue;
+        const double* kij = kf + ((size_t)i * c.ny + j) * c.kx * c.ky * c.kz;
+        double acc[GQY];
 #pragma unroll
-      for (int q = 0; q < QY; ++q) acc[q] = 0.0;
-      const int nplanes = p.kz;  // kernel planes (3-D: z taps; plane mode: summed source planes)
-      for (int dz = 0; dz < nplanes; ++dz) {
-        __syncthreads();
-        // ---- stage the source planes this dz needs (one per output plane)
-        for (int e = tid; e < nzo * hplane; e += THREADS) {
-          const int zi = e / hplane, rem = e % hplane, hxi = rem / p.hy, hyi = rem % p.hy;
-          const int gx = x0 - p.cx + hxi, gy = y0 - p.cy + hyi;
-          const int gz = p.plane ? dz : z0 + zi + dz - p.cz;
-          double v = 0.0;
-          if (gx >= 0 && gx < p.sx && gy >= 0 && gy < p.sy && gz >= 0 && gz < p.sz && z0 + zi < p.sz) {
-            v = p.src[((size_t)gx * p.sy + gy) * p.sz + gz];
-            if (p.detection) v *= p.wx[(size_t)i * p.sx + gx] * p.wy[(size_t)j * p.sy + gy] * wz_at(p, gz);
+        for (int q = 0; q < GQY; ++q) acc[q] = 0.0;
+        for (int dz = 0; dz < c.kz; ++dz) {
+          __syncthreads();
+          for (int e = tid; e < nzo * hplane; e += GEN_THREADS) {
+            const int zi = e / hplane, rem = e % hplane, hxi = rem / P.hy, hyi = rem % P.hy;
+            const int gx = x0 - c.cx + hxi, gy = y0 - c.cy + hyi;
+            const int gz = c.plane ? dz : z0 + zi + dz - c.cz;
+            double v = 0.0;
+            if (gx >= 0 && gx < c.sx && gy >= 0 && gy < c.sy && gz >= 0 && gz < c.sz && z0 + zi < c.sz) {
+              v = c.srcT[((size_t)gz * c.sx + gx) * c.sy + gy];
+              if (P.detection) v *= c.wx[(size_t)i * c.sx + gx] * c.wy[(size_t)j * c.sy + gy] * wz_at(c, f, gz);
+            }
+            halo[e] = v;
           }
-          halo[e] = v;
-        }
-        // ---- stage kernel plane dz (flipped for convolutions), zero padded to kyp
-        for (int e = tid; e < p.kx * p.kyp; e += THREADS) {
-          const int ux = e / p.kyp, uy = e % p.kyp;
-          double v = 0.0;
-          if (uy < p.ky) {
-            const int fx = p.flip ? p.kx - 1 - ux : ux, fy = p.flip ? p.ky - 1 - uy : uy;
-            const int fz = (p.flip && !p.plane) ? p.kz - 1 - dz : dz;
-            v = kij[((size_t)fx * p.ky + fy) * p.kz + fz];
+          for (int e = tid; e < c.kx * P.kyp; e += GEN_THREADS) {
+            const int ux = e / P.kyp, uy = e % P.kyp;
+            const int kp = (c.flip && !c.plane) ? c.kz - 1 - dz : dz;
+            ks[e] = uy < c.ky ? kernel_tap(c, kij, ux, uy, kp) : 0.0;
           }
-          ks[e] = v;
-        }
-        __syncthreads();
-        if (tzi < nzo) {
-          const double* hrow0 = halo + (size_t)tzi * hplane + (size_t)tx * p.hy + tq * QY;
-          for (int ux = 0; ux < p.kx; ++ux) {
-            const double* hrow = hrow0 + (size_t)ux * p.hy;
-            const double* krow = ks + (size_t)ux * p.kyp;
-            double w[2 * QY];
+          __syncthreads();
+          if (tzi < nzo) {
+            const double* hrow0 = halo + (size_t)tzi * hplane + (size_t)tx * P.hy + tq * GQY;
+            for (int ux = 0; ux < c.kx; ++ux) {
+              const double* hrow = hrow0 + (size_t)ux * P.hy;
+              const double* krow = ks + (size_t)ux * P.kyp;
+              double w[2 * GQY];
 #pragma unroll
-            for (int q = 0; q < QY; ++q) w[q] = hrow[q];
-            for (int uy0 = 0; uy0 < p.kyp; uy0 += QY) {
+              for (int q = 0; q < GQY; ++q) w[q] = hrow[q];
+              for (int uy0 = 0; uy0 < P.kyp; uy0 += GQY) {
 #pragma unroll
-              for (int q = 0; q < QY; ++q) w[QY + q] = hrow[uy0 + QY + q];
+                for (int q = 0; q < GQY; ++q) w[GQY + q] = hrow[uy0 + GQY + q];
 #pragma unroll
-              for (int ph = 0; ph < QY; ++ph) {
-                const double kv = krow[uy0 + ph];
+                for (int ph = 0; ph < GQY; ++ph) {
+                  const double kv = krow[uy0 + ph];
 #pragma unroll
-                for (int q = 0; q < QY; ++q) acc[q] = fma(w[q + ph], kv, acc[q]);
+                  for (int q = 0; q < GQY; ++q) acc[q] = fma(w[q + ph], kv, acc[q]);
+                }
+#pragma unroll
+                for (int q = 0; q < GQY; ++q) w[q] = w[GQY + q];
               }
-#pragma unroll
-              for (int q = 0; q < QY; ++q) w[q] = w[QY + q];
             }
           }
         }
-      }
-      // ---- weight the pair's contribution at the output pixel (excitation / native)
-      const int ox = x0 + tx;
+        const int ox = x0 + tx;
 #pragma unroll
-      for (int q = 0; q < QY; ++q) {
-        const int oy = y0 + tq * QY + q;
-        double wgt = 1.0;
-        if (!p.detection) wgt = (ox < p.sx && oy < p.sy) ? p.wx[(size_t)i * p.sx + ox] * p.wy[(size_t)j * p.sy + oy] : 0.0;
-        acc_total[q] = fma(wgt, acc[q], acc_total[q]);
+        for (int q = 0; q < GQY; ++q) {
+          const int oy = y0 + tq * GQY + q;
+          double wgt = 1.0;
+          if (!P.detection)
+            wgt = (ox < c.sx && oy < c.sy) ? c.wx[(size_t)i * c.sx + ox] * c.wy[(size_t)j * c.sy + oy] : 0.0;
+          if (!P.detection && !c.plane) wgt *= (z0 + tzi < c.sz) ? wz_at(c, f, z0 + tzi) : 0.0;
+          acc_total[q] = fma(wgt, acc[q], acc_total[q]);
+        }
       }
     }
   }
   if (tzi >= nzo) return;
   const int ox = x0 + tx, oz = z0 + tzi;
-  if (ox >= p.sx || (!p.plane && oz >= p.sz)) return;
-  const double zw = (!p.detection && !p.plane) ? wz_at(p, oz) : 1.0;
+  if (ox >= c.sx || (!c.plane && oz >= c.sz)) return;
 #pragma unroll
-  for (int q = 0; q < QY; ++q) {
-    const int oy = y0 + tq * QY + q;
-    if (oy >= p.sy) continue;
-    double* dst = p.plane ? p.out + (size_t)ox * p.sy + oy : p.out + ((size_t)ox * p.sy + oy) * p.sz + oz;
-    *dst += zw * acc_total[q];
+  for (int q = 0; q < GQY; ++q) {
+    const int oy = y0 + tq * GQY + q;
+    if (oy >= c.sy) continue;
+    double* dst = c.plane ? c.out + (size_t)ox * c.sy + oy : c.out + ((size_t)ox * c.sy + oy) * c.sz + oz;
+    *dst += acc_total[q];
   }
+}
+
+// Row pitch of the cell kernel's halo planes: at least `need`, chosen so the
+// 16 lanes of each half-warp (rows fastest, QY-wide chunks) read from
+// distinct 8-byte bank pairs.
+int cell_halo_pitch(int need) {
+  int best = need, best_ways = 1 << 30;
+  for (int hy = need; hy < need + 16; ++hy) {
+    int worst = 0;
+    for (int half = 0; half < GROUP / 16; ++half) {
+      int count[16] = {0};
+      for (int u = half * 16; u < half * 16 + 16 && u < TMAX * CH; ++u) {
+        const int chk = u / TMAX, row = u % TMAX;
+        worst = std::max(worst, ++count[(row * hy + chk * QY) % 16]);
+      }
+    }
+    if (worst < best_ways) {
+      best_ways = worst;
+      best = hy;
+    }
+  }
+  return best;
+}
+
+Common common_params(const mm_local_desc* d, const double* srcT, const double* zweight, double* out) {
+  Common c{};
+  c.sx = d->sx; c.sy = d->sy; c.sz = d->sz;
+  c.kx = d->kx; c.ky = d->ky; c.kz = d->kz;
+  c.nx = d->nodes_x; c.ny = d->nodes_y; c.nf = d->nfields;
+  c.kern = d->kernels; c.wx = d->wx; c.wy = d->wy; c.wz = zweight;
+  c.srcT = srcT;
+  c.out = out;
+  c.flip = !d->correlate;  // convolutions become correlations with the flipped kernel
+  c.plane = d->plane;
+  // correlation offset of the staged kernel: K/2 (correlate) or K-1-K/2 (flipped)
+  c.cx = d->correlate ? d->kx / 2 : d->kx - 1 - d->kx / 2;
+  c.cy = d->correlate ? d->ky / 2 : d->ky - 1 - d->ky / 2;
+  c.cz = d->correlate ? d->kz / 2 : d->kz - 1 - d->kz / 2;
+  return c;
 }
 
 }  // namespace
 }  // namespace mm
 
-extern "C" size_t mm_local_render_workspace_size(const mm_local_desc* desc) {
-  (void)desc;
-  return 0;  // the render needs no workspace
+extern "C" int mm_local_tiles(const double* w, int nodes, int n, int max_len, int* table, int capacity) {
+  using namespace mm;
+  MM_CHECK_ARG(w && nodes >= 1 && n >= 1, "bad weight table");
+  if (max_len <= 0 || max_len > TMAX) max_len = TMAX;
+  // active node set per pixel
+  std::vector<int> sets((size_t)n * kMaxActive, -1);
+  std::vector<int> counts(n, 0);
+  for (int x = 0; x < n; ++x)
+    for (int i = 0; i < nodes; ++i)
+      if (w[(size_t)i * n + x] != 0.0) {
+        if (counts[x] == kMaxActive) {
+          set_error("pixel %d has more than %d nodes with nonzero weight", x, kMaxActive);
+          return MM_ERR_UNSUPPORTED;
+        }
+        sets[(size_t)x * kMaxActive + counts[x]++] = i;
+      }
+  int ntiles = 0;
+  for (int a = 0; a < n;) {
+    int b = a + 1;
+    while (b < n && counts[b] == counts[a] &&
+           std::equal(&sets[(size_t)b * kMaxActive], &sets[(size_t)b * kMaxActive] + kMaxActive,
+                      &sets[(size_t)a * kMaxActive]))
+      ++b;
+    // [a, b) shares one node set; split it evenly into pieces of <= max_len
+    const int len = b - a, pieces = (len + max_len - 1) / max_len;
+    for (int k = 0; k < pieces; ++k) {
+      const int s = a + (int)((long long)len * k / pieces), e = a + (int)((long long)len * (k + 1) / pieces);
+      if (counts[a] > 0) {  // pixels with no active node get no tile (their sum is zero)
+        if (table && ntiles < capacity) {
+          int* t = table + (size_t)ntiles * kTileInts;
+          t[0] = s;
+          t[1] = e - s;
+          t[2] = counts[a];
+          for (int m = 0; m < kMaxActive; ++m) t[3 + m] = sets[(size_t)a * kMaxActive + m];
+          t[7] = 0;
+        }
+        ++ntiles;
+      }
+    }
+    a = b;
+  }
+  return ntiles;
+}
+
+extern "C" size_t mm_local_render_workspace_size(const mm_local_desc* d) {
+  if (!d || d->sx < 1 || d->sy < 1 || d->sz < 1) return 0;
+  return ((size_t)d->sx * d->sy * d->sz * sizeof(double) + 255) / 256 * 256;
 }
 
 extern "C" int mm_local_render(const mm_local_desc* d, const double* source, const double* zweight, double* out,
                                void* workspace, size_t workspace_bytes, void* stream) {
   using namespace mm;
-  (void)workspace;
-  (void)workspace_bytes;
   MM_CHECK_ARG(d && source && out && d->kernels && d->wx && d->wy, "NULL pointer");
   MM_CHECK_ARG(d->sx >= 1 && d->sy >= 1 && d->sz >= 1 && d->kx >= 1 && d->ky >= 1 && d->kz >= 1 && d->nodes_x >= 1 &&
-                   d->nodes_y >= 1,
+                   d->nodes_y >= 1 && d->nfields >= 1,
                "bad local-render sizes");
   MM_CHECK_ARG(!d->plane || d->kz == d->sz, "plane mode needs kernel depth == source depth (%d vs %d)", d->kz, d->sz);
+  MM_CHECK_ARG(!d->plane || (d->nfields == 1 && !zweight), "plane mode renders one field with pre-weighted source");
+  MM_CHECK_ARG(zweight || d->nfields == 1, "several fields need their depth weights");
   MM_CHECK_ARG(d->nodes_x <= kMaxNodes && d->nodes_y <= kMaxNodes, "at most %d field nodes per axis", kMaxNodes);
-  LocalP p{};
-  p.sx = d->sx; p.sy = d->sy; p.sz = d->sz;
-  p.kx = d->kx; p.ky = d->ky; p.kz = d->kz;
-  p.nx = d->nodes_x; p.ny = d->nodes_y;
-  p.kyp = (d->ky + QY - 1) / QY * QY;
-  p.hx = TX + p.kx - 1;
-  p.hy = TY + p.kyp - 1 + QY;  // the window reads QY past the last tap
-  p.kern = d->kernels; p.wx = d->wx; p.wy = d->wy; p.wz = zweight;
-  p.detection = d->detection;
-  p.flip = !d->correlate;  // convolutions become correlations with the flipped kernel
-  p.plane = d->plane;
-  // correlation offset of the staged kernel: K/2 (correlate) or K-1-K/2 (flipped)
-  p.cx = d->correlate ? d->kx / 2 : d->kx - 1 - d->kx / 2;
-  p.cy = d->correlate ? d->ky / 2 : d->ky - 1 - d->ky / 2;
-  p.cz = d->correlate ? d->kz / 2 : d->kz - 1 - d->kz / 2;
-  p.out = out;
-  p.src = source;
-  const size_t smem = ((size_t)TZ * p.hx * p.hy + (size_t)p.kx * p.kyp) * sizeof(double);
+  const size_t need = mm_local_render_workspace_size(d);
+  MM_CHECK_ARG(workspace && workspace_bytes >= need, "workspace too small: %zu bytes given, %zu needed",
+               workspace_bytes, need);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  double* srcT = static_cast<double*>(workspace);
+  transpose_kernel<<<dim3(d->sx, (d->sy + 31) / 32), 256, 0, s>>>(source, d->sx, d->sy, d->sz, srcT);
+  MM_CHECK_LAUNCH("local render transpose");
+  const Common c = common_params(d, srcT, zweight, out);
+  if (!d->detection) {
+    MM_CHECK_ARG(d->tiles_x && d->tiles_y && d->ntiles_x >= 0 && d->ntiles_y >= 0,
+                 "excitation/native render needs the mm_local_tiles tables");
+    if (d->ntiles_x == 0 || d->ntiles_y == 0) return MM_OK;  // no active node anywhere
+    CellP P{};
+    P.c = c;
+    P.tx = d->tiles_x;
+    P.ty = d->tiles_y;
+    P.ntx = d->ntiles_x;
+    P.nty = d->ntiles_y;
+    P.hx = TMAX + d->kx - 1;
+    P.hy = cell_halo_pitch((CH + (d->ky + QY - 1) / QY) * QY);
+    P.kplanes = d->plane ? TZC : 1;
+    const size_t smem = ((size_t)TZC * P.hx * P.hy + (size_t)P.kplanes * PG * d->kx * d->ky) * sizeof(double);
+    const size_t red = (size_t)(TZC - 1) * GROUP * QY * sizeof(double);
+    const size_t bytes = std::max(smem, red);
+    MM_CHECK_ARG(bytes <= 227 * 1024, "kernel %dx%d too large for the shared-memory tile (%zu bytes)", d->kx, d->ky,
+                 bytes);
+    MM_CHECK_CUDA(cudaFuncSetAttribute(cell_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes),
+                  "cudaFuncSetAttribute(local cell render)");
+    const long long tiles = (long long)d->ntiles_x * d->ntiles_y;
+    MM_CHECK_ARG(tiles < (1ll << 31), "too many tiles");
+    const int zblocks = d->plane ? 1 : (d->sz + TZC - 1) / TZC;
+    cell_kernel<<<dim3((unsigned)tiles, zblocks), CELL_THREADS, bytes, s>>>(P);
+    MM_CHECK_LAUNCH("local cell render");
+    return MM_OK;
+  }
+  GenP P{};
+  P.c = c;
+  P.detection = d->detection;
+  P.kyp = (d->ky + GQY - 1) / GQY * GQY;
+  P.hx = TX + d->kx - 1;
+  P.hy = TY + P.kyp - 1 + GQY;  // the window reads GQY past the last tap
+  const size_t smem = ((size_t)TZ * P.hx * P.hy + (size_t)d->kx * P.kyp) * sizeof(double);
   MM_CHECK_ARG(smem <= 227 * 1024, "kernel %dx%d too large for the shared-memory tile (%zu bytes)", d->kx, d->ky, smem);
-  MM_CHECK_CUDA(cudaFuncSetAttribute(local_render_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+  MM_CHECK_CUDA(cudaFuncSetAttribute(generic_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
                 "cudaFuncSetAttribute(local render)");
   const int tiles = ((d->sx + TX - 1) / TX) * ((d->sy + TY - 1) / TY);
   const int zblocks = d->plane ? 1 : (d->sz + TZ - 1) / TZ;
-  local_render_kernel<<<dim3(tiles, zblocks), THREADS, smem, static_cast<cudaStream_t>(stream)>>>(p);
+  generic_kernel<<<dim3(tiles, zblocks), GEN_THREADS, smem, s>>>(P);
   MM_CHECK_LAUNCH("local render");
   return MM_OK;
 }

@@ -1,5 +1,11 @@
-"""Depth-dependent PSF bank (maomi/rana/depth.py:9-69): one complete XYZ
-FullFieldPSF per focal depth, linear depth weights, ``maomi.depth_psf_bank.v1``."""
+"""Depth banks of local-PSF fields: ``DepthPSFBank`` (maomi/rana/depth.py:9-69).
+
+A bank pairs focal depths (micrometres, >= 0, strictly increasing, at least
+two) with one complete XYZ ``FullFieldPSF`` per depth.  All fields must be
+interchangeable apart from their kernel values: same kernel shape, lateral
+nodes, pitch, operator and wavelength.  A renderer weights the fields
+linearly in depth (``depth_weights``).  Files use ``maomi.depth_psf_bank.v1``.
+"""
 
 import json
 from dataclasses import dataclass
@@ -12,6 +18,23 @@ from .fields import FullFieldPSF
 SCHEMA = "maomi.depth_psf_bank.v1"
 
 
+def _same_layout(a, b):
+    return (a.kernels.shape == b.kernels.shape and a.voxel_size_um == b.voxel_size_um and a.operator == b.operator
+            and a.wavelength_nm == b.wavelength_nm and np.array_equal(a.x_um, b.x_um)
+            and np.array_equal(a.y_um, b.y_um))
+
+
+def depth_weights(depths_um, z_um):
+    """Linear interpolation weights (len(depths), len(z)) between the two
+    depth nodes bracketing each plane centre: the hat functions of the depth
+    nodes, so every column sums to one and has at most two nonzero entries.
+    The planes must lie within [depths[0], depths[-1]]."""
+    d = np.asarray(depths_um, float)
+    z = np.atleast_1d(np.asarray(z_um, float))
+    hats = np.eye(len(d))
+    return np.stack([np.interp(z, d, hats[k]) for k in range(len(d))])
+
+
 @dataclass(frozen=True)
 class DepthPSFBank:
     depths_um: np.ndarray
@@ -20,16 +43,15 @@ class DepthPSFBank:
     def __post_init__(self):
         z = np.array(self.depths_um, dtype=float, copy=True)
         fields = tuple(self.fields)
-        if z.ndim != 1 or len(z) < 2 or (np.diff(z) <= 0).any() or not np.isfinite(z).all() or (z < 0).any():
-            raise ValueError("A depth bank requires >= 2 increasing nonnegative finite depths")
-        if len(fields) != len(z) or any(not isinstance(f, FullFieldPSF) or f.kernels.ndim != 5 for f in fields):
-            raise ValueError("One complete XYZ-kernel FullFieldPSF per depth is required")
-        first = fields[0]
-        for f in fields[1:]:
-            if (f.kernels.shape != first.kernels.shape or f.voxel_size_um != first.voxel_size_um
-                    or f.operator != first.operator or f.wavelength_nm != first.wavelength_nm
-                    or not np.array_equal(f.x_um, first.x_um) or not np.array_equal(f.y_um, first.y_um)):
-                raise ValueError("Depth fields must share shape, XY nodes, pitch, operator and wavelength")
+        if z.ndim != 1 or z.size < 2 or not np.all(np.isfinite(z)) or np.any(z < 0) or not np.all(z[1:] > z[:-1]):
+            raise ValueError("depths_um: a bank needs at least two strictly increasing, finite, nonnegative depths")
+        if len(fields) != z.size:
+            raise ValueError(f"{z.size} depths but {len(fields)} fields: give one field per depth")
+        if not all(isinstance(f, FullFieldPSF) and f.kernels.ndim == 5 for f in fields):
+            raise ValueError("every depth needs a FullFieldPSF with XYZ kernels")
+        if not all(_same_layout(fields[0], f) for f in fields[1:]):
+            raise ValueError("the fields of a bank must agree in kernel shape, lateral nodes, pitch, operator "
+                             "and wavelength")
         z.setflags(write=False)
         object.__setattr__(self, "depths_um", z)
         object.__setattr__(self, "fields", fields)
@@ -46,23 +68,38 @@ class DepthPSFBank:
     def wavelength_nm(self):
         return self.fields[0].wavelength_nm
 
+    @classmethod
+    def from_provider(cls, provider, x_um, y_um, depths_um, *, voxel_size_um, wavelength_nm, operator="excitation",
+                      provenance=None):
+        """Bank sampled from ``provider(x_um, y_um, depth_um) -> kernel``; each
+        field's provenance records its focal depth.  maomi/rana/depth.py:44-48."""
+        def at_depth(depth):
+            return FullFieldPSF.from_provider(lambda x, y: provider(x, y, depth), x_um, y_um,
+                                              voxel_size_um=voxel_size_um, wavelength_nm=wavelength_nm,
+                                              operator=operator,
+                                              provenance=dict(provenance or {}, focal_depth_um=depth))
+        return cls(depths_um, tuple(at_depth(float(d)) for d in np.asarray(depths_um, float)))
+
     def save(self, path):
         p = Path(path)
         p.parent.mkdir(parents=True, exist_ok=True)
-        f = self.fields[0]
+        head = self.fields[0]
         np.savez_compressed(p, schema=SCHEMA, depths_um=self.depths_um,
-                            kernels=np.stack([x.kernels for x in self.fields]), x_um=f.x_um, y_um=f.y_um,
-                            voxel_size_um=f.voxel_size_um, wavelength_nm=f.wavelength_nm, operator=f.operator,
-                            provenance=json.dumps([x.provenance for x in self.fields], allow_nan=False))
+                            kernels=np.stack([f.kernels for f in self.fields]), x_um=head.x_um, y_um=head.y_um,
+                            voxel_size_um=head.voxel_size_um, wavelength_nm=head.wavelength_nm,
+                            operator=head.operator,
+                            provenance=json.dumps([f.provenance for f in self.fields], allow_nan=False))
 
     @classmethod
     def load(cls, path):
         with np.load(path, allow_pickle=False) as d:
-            if str(d["schema"]) != SCHEMA:
-                raise ValueError("Unsupported depth-bank schema")
+            found = str(d["schema"]) if "schema" in d.files else "<none>"
+            if found != SCHEMA:
+                raise ValueError(f"not a {SCHEMA} file (schema {found})")
             meta = json.loads(str(d["provenance"]))
-            if len(meta) != len(d["depths_um"]) or len(d["kernels"]) != len(d["depths_um"]):
-                raise ValueError("Malformed depth bank: inconsistent depth, kernel or provenance counts")
-            return cls(d["depths_um"], tuple(
-                FullFieldPSF(k, d["x_um"], d["y_um"], tuple(d["voxel_size_um"]), float(d["wavelength_nm"]),
-                             str(d["operator"]), m) for k, m in zip(d["kernels"], meta)))
+            count = len(d["depths_um"])
+            if len(meta) != count or len(d["kernels"]) != count:
+                raise ValueError(f"malformed depth bank: {count} depths, {len(d['kernels'])} kernel sets, "
+                                 f"{len(meta)} provenance records")
+            common = (d["x_um"], d["y_um"], tuple(d["voxel_size_um"]), float(d["wavelength_nm"]), str(d["operator"]))
+            return cls(d["depths_um"], tuple(FullFieldPSF(k, *common, m) for k, m in zip(d["kernels"], meta)))

@@ -1,190 +1,257 @@
-"""``RanaOperator`` on the GPU (maomi/rana/operator.py:20-167).
+"""Spatially varying local-PSF operator on the GPU: ``RanaOperator``.
 
-The same node weights (C1 smoothstep hats between XY nodes, linear depth
-weights), the same detection / excitation / native conventions and the same
-``static`` and ``scan_slab`` entry points; every projection runs through
-``mm_local_render`` in FP64, with the depth weight of a bank field applied
-inside the render launch."""
+Drop-in for maomi/rana/operator.py:20-167 (constructor, ``static``,
+``scan_slab``, ``clear_cache``, ``cache_info``, ``physical_tail``, and the
+attributes the movie and adapter code read: ``bank``, ``fields``, ``field``,
+``kernel_shape``, ``voxel_size_um``, ``origin_um``, ``z_origin_um``,
+``native``, ``device``, ``settings``).
 
-from collections import OrderedDict
+How it renders:
+
+* lateral weights: every output pixel centre gets the C1 smoothstep hat
+  weights t^2 (3 - 2 t) of the two nodes bracketing it on each axis
+  (maomi/rana/operator.py:10-17), so at most 2 x 2 node pairs act per pixel;
+* depth weights: the fields of a ``DepthPSFBank`` are mixed linearly in the
+  depth of each plane centre (operator.py:91-97);
+* ``static``: ONE ``mm_local_render`` launch for the whole bank, the depth
+  weights applied per output plane (excitation / native) or per source plane
+  (detection) inside the kernel, then the result clipped at zero;
+* ``scan_slab``: per field a plane-mode render of the slab, the kernels
+  mirrored in depth for detection and binned by ``scan_avg``
+  (operator.py:136-167).
+
+Arithmetic is FP64 throughout, as in the reference.
+"""
 
 import numpy as np
 
-from .depth import DepthPSFBank
-from .fields import FullFieldPSF
 from ._backends import get_backend
-from ._fft import LocalFFTPlan
+from ._fft import DeviceRender
+from .depth import DepthPSFBank, depth_weights
+from .fields import FullFieldPSF
+
+_COVER_TOL = 1e-10
 
 
 def _axis_weights(nodes, positions):
-    """C1 smoothstep t^2(3-2t) between the two nodes bracketing each position."""
-    ids = np.clip(np.searchsorted(nodes, positions, side="right") - 1, 0, len(nodes) - 2)
-    t = np.clip((positions - nodes[ids]) / (nodes[ids + 1] - nodes[ids]), 0, 1)
-    t = t * t * (3 - 2 * t)
-    w = np.zeros((len(nodes), len(positions)))
-    cols = np.arange(len(positions))
-    w[ids, cols] = 1 - t
-    w[ids + 1, cols] = t
+    """(len(nodes), len(positions)) smoothstep hat weights: a position between
+    nodes a and a+1 at fraction t gives node a 1 - s(t) and node a+1 s(t),
+    s(t) = t^2 (3 - 2 t); positions beyond the end nodes clamp to them."""
+    nodes = np.asarray(nodes, float)
+    pos = np.asarray(positions, float)
+    a = np.searchsorted(nodes, pos, side="right") - 1
+    a = np.minimum(np.maximum(a, 0), len(nodes) - 2)
+    t = (pos - nodes[a]) / (nodes[a + 1] - nodes[a])
+    t = np.minimum(np.maximum(t, 0.0), 1.0)
+    s = t * t * (3 - 2 * t)
+    w = np.zeros((len(nodes), len(pos)))
+    col = np.arange(len(pos))
+    w[a, col] = 1 - s
+    w[a + 1, col] = s
     return w
 
 
-def _resolve(field):
-    if isinstance(field, (FullFieldPSF, DepthPSFBank)):
-        return field
-    build = getattr(field, "build_field", None)
+def resolve_field(source):
+    """A FullFieldPSF / DepthPSFBank, or what a provider's build_field() returns."""
+    if isinstance(source, (FullFieldPSF, DepthPSFBank)):
+        return source
+    build = getattr(source, "build_field", None)
     if not callable(build):
-        raise TypeError("Supply FullFieldPSF, DepthPSFBank or a PSFProvider with build_field()")
-    out = build()
-    if not isinstance(out, (FullFieldPSF, DepthPSFBank)):
-        raise TypeError("PSFProvider.build_field() must return FullFieldPSF or DepthPSFBank")
+        raise TypeError("expected a FullFieldPSF, a DepthPSFBank or a provider with build_field()")
+    built = build()
+    if not isinstance(built, (FullFieldPSF, DepthPSFBank)):
+        raise TypeError("a provider's build_field() must return a FullFieldPSF or a DepthPSFBank")
+    return built
+
+
+def _mirror_depth(kernels, center):
+    """Kernel planes reflected about ``center`` (plane p takes plane
+    2*center - p); planes whose mirror falls outside the kernel are zero."""
+    out = np.zeros_like(kernels)
+    kz = kernels.shape[-1]
+    for p in range(kz):
+        src = 2 * center - p
+        if 0 <= src < kz:
+            out[..., p] = kernels[..., src]
     return out
+
+
+def _bin_planes(a, width):
+    """Sums over consecutive groups of ``width`` planes of the last axis."""
+    return np.stack([a[..., s:s + width].sum(-1) for s in range(0, a.shape[-1], width)], -1)
 
 
 class RanaOperator:
     def __init__(self, field, *, native=False, origin_um=(0., 0.), z_origin_um=0., device="cuda"):
-        field = _resolve(field)
-        self.bank = field if isinstance(field, DepthPSFBank) else None
-        self.fields = field.fields if self.bank is not None else (field,)
-        if any(not isinstance(f, FullFieldPSF) or f.kernels.ndim != 5 for f in self.fields):
-            raise TypeError("The acquisition add-on requires complete XYZ-kernel fields")
+        source = resolve_field(field)
+        if isinstance(source, DepthPSFBank):
+            self.bank, self.fields = source, tuple(source.fields)
+        else:
+            self.bank, self.fields = None, (source,)
+        if not all(isinstance(f, FullFieldPSF) and f.kernels.ndim == 5 for f in self.fields):
+            raise TypeError("the local operator renders XYZ kernels only (FullFieldPSF with 5-D kernels)")
         self.field = self.fields[0]
         self.kernel_shape = self.field.kernels.shape[2:]
         self.voxel_size_um = self.field.voxel_size_um
-        self.origin_um, self.z_origin_um = np.asarray(origin_um, float), float(z_origin_um)
-        self.native, self.device = native, str(device)
-        if (self.origin_um.shape != (2,) or not np.isfinite(self.origin_um).all()
-                or not np.isfinite(self.z_origin_um)):
-            raise ValueError("Supply finite XY and Z origins")
+        self.origin_um = np.asarray(origin_um, dtype=float)
+        self.z_origin_um = float(z_origin_um)
+        if self.origin_um.shape != (2,) or not np.all(np.isfinite(self.origin_um)) or not np.isfinite(self.z_origin_um):
+            raise ValueError("origin_um needs two finite values and z_origin_um one")
+        self.native, self.device = bool(native), str(device)
         self._backend = get_backend(self.device)
-        self._cache = {}
-        self._plans = OrderedDict()
-        self._scan_kernels = {}
-        self.settings = {"enabled": True, "operator": "native_scan" if native else self.field.operator,
-                         "interpolation": "positive local cubic tensor weights",
-                         "field_nodes": list(self.field.kernels.shape[:2]), "kernel_shape": list(self.kernel_shape),
-                         "depth_nodes_um": None if self.bank is None else self.bank.depths_um.tolist(),
-                         "shared_psf_fallback": False, "device": self.device,
-                         "provenance": [f.provenance for f in self.fields]}
+        self._lateral = {}      # (X, Y) -> host weight tables (wx, wy)
+        self._static = {}       # volume shape -> DeviceRender of the whole bank
+        self._planes = {}       # (shape, field, scan_avg, detection) -> DeviceRender of one field
+        self._reuses = 0
+        mode = "native_scan" if self.native else self.field.operator
+        self.settings = {
+            "enabled": True, "operator": mode,
+            "interpolation": "positive local cubic tensor weights",
+            "field_nodes": list(self.field.kernels.shape[:2]), "kernel_shape": list(self.kernel_shape),
+            "depth_nodes_um": None if self.bank is None else self.bank.depths_um.tolist(),
+            "shared_psf_fallback": False, "device": self.device,
+            "renderer": "maomi_b200 mm_local_render (FP64 direct sum over the active node pairs)",
+            "provenance": [f.provenance for f in self.fields],
+        }
 
+    # --------------------------------------------------------------- weights
     @property
     def _detection(self):
-        return not self.native and self.field.operator == "detection"
+        return self.field.operator == "detection" and not self.native
 
     @property
     def _correlate(self):
-        return not self.native and self.field.operator == "excitation"
+        return self.field.operator == "excitation" and not self.native
 
     def _weights(self, shape):
-        shape = tuple(shape[:2])
-        if shape not in self._cache:
-            pitch = np.array(self.voxel_size_um[:2])
-            lower = np.array([self.field.x_um[0], self.field.y_um[0]])
-            upper = np.array([self.field.x_um[-1], self.field.y_um[-1]])
-            if ((self.origin_um < lower - 1e-10).any()
-                    or (self.origin_um + np.array(shape) * pitch > upper + 1e-10).any()):
-                raise ValueError("RANA field must cover the entire acquisition FOV")
-            coords = [o + (np.arange(n) + .5) * p for o, n, p in zip(self.origin_um, shape, pitch)]
-            self._cache[shape] = tuple(_axis_weights(nodes, q)
-                                       for nodes, q in zip((self.field.x_um, self.field.y_um), coords))
-        return self._cache[shape]
+        """Lateral hat weights of the pixel centres of an (X, Y, ...) volume."""
+        key = tuple(int(v) for v in shape[:2])
+        if key not in self._lateral:
+            pitch = np.asarray(self.voxel_size_um[:2], float)
+            nodes = (self.field.x_um, self.field.y_um)
+            lo = np.array([n[0] for n in nodes])
+            hi = np.array([n[-1] for n in nodes])
+            end = self.origin_um + np.asarray(key) * pitch
+            if np.any(self.origin_um < lo - _COVER_TOL) or np.any(end > hi + _COVER_TOL):
+                raise ValueError("the PSF field's nodes must cover the whole acquisition field of view")
+            centres = [o + (np.arange(n) + 0.5) * p for o, n, p in zip(self.origin_um, key, pitch)]
+            self._lateral[key] = tuple(_axis_weights(nd, c) for nd, c in zip(nodes, centres))
+        return self._lateral[key]
 
-    def _depth_weights(self, z):
+    def _depth_weights(self, z_um):
+        """(fields, planes) depth weights of plane centres at ``z_um``."""
+        z = np.atleast_1d(np.asarray(z_um, float))
         if self.bank is None:
-            return np.ones((1, np.size(z)))
-        z = np.atleast_1d(z)
-        if (z < self.bank.depths_um[0] - 1e-10).any() or (z > self.bank.depths_um[-1] + 1e-10).any():
-            raise ValueError("RANA depth bank does not cover the requested acquisition depths")
-        return np.stack([np.interp(z, self.bank.depths_um, row) for row in np.eye(len(self.fields))])
+            return np.ones((1, z.size))
+        d = self.bank.depths_um
+        if np.any(z < d[0] - _COVER_TOL) or np.any(z > d[-1] + _COVER_TOL):
+            raise ValueError("the depth bank does not span the requested plane depths")
+        return depth_weights(d, z)
 
+    def _plane_centres(self, first, count):
+        return self.z_origin_um + (first + np.arange(count) + 0.5) * self.voxel_size_um[2]
+
+    # ----------------------------------------------------------------- cache
     def clear_cache(self):
-        self._plans.clear()
-        self._scan_kernels.clear()
-        self._cache.clear()
+        """Drop the device-resident kernels, weights and workspaces."""
+        self._static.clear()
+        self._planes.clear()
+        self._lateral.clear()
 
     @property
     def cache_info(self):
-        names = ("kernel_fft_builds", "cache_hits")
-        return dict(plans=len(self._plans), fft_bytes=sum(p.cache_bytes for p in self._plans.values()),
-                    **{k: sum(p.stats[k] for p in self._plans.values()) for k in names})
+        renders = list(self._static.values()) + list(self._planes.values())
+        return dict(plans=len(renders), fft_bytes=0, kernel_fft_builds=0, cache_hits=self._reuses)
 
-    def _plan(self, shape, kernels, plane):
-        key = (tuple(shape), id(kernels), plane)
-        if key not in self._plans:
-            limit = max(2, 2 * len(self.fields))
-            while len(self._plans) >= limit:
-                self._plans.popitem(last=False)[1].clear()
-            self._plans[key] = LocalFFTPlan(shape, kernels, self._weights(shape), plane=plane,
-                                            detection=self._detection, correlate=self._correlate,
-                                            device=self.device, cache_mb=256 / limit)
-        self._plans.move_to_end(key)
-        return self._plans[key]
+    def _cached(self, table, key, build):
+        if key in table:
+            self._reuses += 1
+        else:
+            table[key] = build()
+        return table[key]
 
-    def _finish(self, result):
-        return np.maximum(self._backend.to_numpy(result), 0.)
-
+    # ------------------------------------------------------------------ maths
     @staticmethod
     def physical_tail(values):
-        """Remove negative intensity ringing without changing integrated gain."""
+        """Clip negative ringing of a tail intensity to zero and rescale the rest
+        so the integrated gain is unchanged; the input must be real, finite and
+        of positive total."""
         a = np.asarray(values)
-        if np.iscomplexobj(a) or not np.isfinite(a).all() or a.sum(dtype=float) <= 0:
-            raise ValueError("Tail intensity must have positive finite integrated gain")
-        if np.any(a < 0):
-            positive = np.maximum(a, 0)
-            return positive * (a.sum(dtype=float) / positive.sum(dtype=float))
-        return a
+        total = a.sum(dtype=float) if not np.iscomplexobj(a) else np.nan
+        if np.iscomplexobj(a) or not np.all(np.isfinite(a)) or not total > 0:
+            raise ValueError("a tail intensity must be real and finite with a positive integrated gain")
+        if not np.any(a < 0):
+            return a
+        kept = np.maximum(a, 0)
+        return kept * (total / kept.sum(dtype=float))
 
     @staticmethod
     def _density(volume):
         if np.iscomplexobj(volume):
-            raise ValueError("Fluorescence must be real")
+            raise ValueError("fluorescence must be a real density")
         a = np.asarray(volume, dtype=float)
-        if a.ndim != 3 or not np.isfinite(a).all() or (a < 0).any():
-            raise ValueError("Supply finite nonnegative XYZ fluorescence")
+        if a.ndim != 3 or not np.all(np.isfinite(a)) or np.any(a < 0):
+            raise ValueError("fluorescence must be a finite, nonnegative (X, Y, Z) volume")
         return a
 
+    def _finish(self, result):
+        return np.maximum(self._backend.to_numpy(result), 0.0)
+
+    # ------------------------------------------------------------ rendering
     def static(self, volume):
-        """Whole-volume render: detection weights sources per depth before the
-        local convolution, excitation weights the local correlation after."""
+        """Render a whole volume: every plane through the depth-weighted fields."""
         a = self._density(volume)
-        z = self.z_origin_um + (np.arange(a.shape[2]) + .5) * self.voxel_size_um[2]
-        weights = self._depth_weights(z)
-        src = self._backend.array(a)
-        result = self._backend.zeros(a.shape)
-        for f, w in zip(self.fields, weights):
-            if not np.any(w):
-                continue
-            self._plan(a.shape, f.kernels, False)(src, zweight=w, out=result)
-        return self._finish(result)
+        wz = self._depth_weights(self._plane_centres(0, a.shape[2]))
+
+        def build():
+            wx, wy = self._weights(a.shape)
+            kern = np.stack([f.kernels for f in self.fields])
+            return DeviceRender(a.shape, kern, wx, wy, plane=False, detection=self._detection,
+                                correlate=self._correlate, device=self.device)
+
+        render = self._cached(self._static, a.shape, build)
+        b = self._backend
+        out = b.zeros(a.shape)
+        render(b.array(a), zweight=wz if self.bank is not None else None, out=out)
+        return self._finish(out)
 
     def scan_slab(self, slab, *, z_start=0, scan_avg=1):
+        """Image of one focal slab (depth = kernel depth) starting at plane
+        ``z_start``: the 2-D operator summed over the slab's planes, averaged
+        in groups of ``scan_avg`` planes."""
         a = self._density(slab)
-        if a.shape[2] != self.kernel_shape[2]:
-            raise ValueError("Focal slab depth must match the RANA kernel")
-        if not isinstance(scan_avg, (int, np.integer)) or scan_avg < 1:
+        kz = self.kernel_shape[2]
+        if a.shape[2] != kz:
+            raise ValueError(f"the slab must have the kernel's depth ({kz} planes), got {a.shape[2]}")
+        if isinstance(scan_avg, bool) or not isinstance(scan_avg, (int, np.integer)) or scan_avg < 1:
             raise ValueError("scan_avg must be a positive integer")
-        center = self.kernel_shape[2] // 2
-        z = self.z_origin_um + (z_start + np.arange(a.shape[2]) + .5) * self.voxel_size_um[2]
-        detection = self._detection
-        weights = self._depth_weights(z if detection else [z[center]])
-        starts = np.arange(0, a.shape[2], scan_avg)
-        dev = self._backend.array(a)
-        result = self._backend.zeros(a.shape[:2])
-        for index, (f, w) in enumerate(zip(self.fields, weights)):
+        width = int(scan_avg)
+        centre = kz // 2
+        z = self._plane_centres(z_start, kz)
+        detect = self._detection
+        # detection weights each source plane by its own depth; excitation and
+        # native scans weight the whole slab by the depth of its centre plane
+        wz = self._depth_weights(z if detect else z[centre:centre + 1])
+        b = self._backend
+        src = b.array(a)
+        out = b.zeros(a.shape[:2])
+        wx, wy = self._weights(a.shape)
+        for index, (f, w) in enumerate(zip(self.fields, wz)):
             if not np.any(w):
                 continue
-            source = dev * self._backend.array(w) if detection else dev
-            key = (index, scan_avg, detection)
-            if key not in self._scan_kernels:
-                kernels = f.kernels
-                if detection:
-                    ids = 2 * center - np.arange(a.shape[2])
-                    kernels = np.take(kernels, np.minimum(ids, a.shape[2] - 1), axis=-1).copy()
-                    kernels[..., ids >= a.shape[2]] = 0
-                if scan_avg > 1:
-                    kernels = np.add.reduceat(kernels, starts, axis=-1)
-                self._scan_kernels[key] = kernels
-            if scan_avg > 1:
-                source = self._backend.group_sum(source, starts, scan_avg)
-            piece = self._plan(tuple(source.shape), self._scan_kernels[key], True)(source)
-            result += piece * (1 if detection else float(w[0]))
-        return self._finish(result)
+            source = src * b.array(w) if detect else src
+            if width > 1:
+                source = b.group_sum(source, range(0, kz, width), width)
+            nz = int(source.shape[2])
+
+            def build(f=f):
+                k = _mirror_depth(f.kernels, centre) if detect else f.kernels
+                if width > 1:
+                    k = _bin_planes(k, width)
+                return DeviceRender((a.shape[0], a.shape[1], nz), k[None], wx, wy, plane=True,
+                                    detection=detect, correlate=self._correlate, device=self.device)
+
+            render = self._cached(self._planes, (a.shape, index, width, detect), build)
+            piece = render(source)
+            out += piece if detect else piece * float(w[0])
+        return self._finish(out)

@@ -111,3 +111,29 @@ def psf_bank_kernels(nodes=(16, 16), kernel=(33, 33, 9), depths=4, seed=5):
                 xr = X + tilt * Z
                 out[d, i, j] = gain * np.exp(-(xr / sx) ** 2 - (Y / sy) ** 2 - (Z / sz) ** 2) + 1e-6
     return out.astype(np.float32)
+
+
+def propagated_psf_bank(cls, *, nodes=16, kernel=(33, 33, 9), depths_um=(0.0, 16.0 / 3, 32.0 / 3, 16.0),
+                        fov_um=256.0, base_depth_um=30.0, sigma=3.0, rms=0.015, seed=21, device="cuda"):
+    """Depth bank of local excitation PSFs made by the optical stage itself.
+
+    For each bank depth d the stage runs on a tissue block of ``fov_um`` x
+    ``fov_um`` x 16 um at 1 um voxels (vres 1, no supersampling) focused at ``base_depth_um + d``,
+    with scattering screens of the benchmark recipe (``sigma`` voxels, RMS
+    ``rms``), over a ``nodes`` x ``nodes`` lattice of sites; each site's focal
+    |E|^4 PSF (``kernel[0] + 1`` x ``kernel[1] + 1`` x ``kernel[2]`` at 1 um)
+    is trimmed by its first row and column to ``kernel``, which keeps the
+    focus at index ``kernel // 2``.  Returns (kernels (depths, nodes, nodes,
+    kx, ky, kz) float64, node positions in um (shared by x and y), depths)."""
+    from .fixed import field_shapes, run_stage
+    kx, ky, kz = kernel
+    ticks = np.round(np.linspace(0.0, fov_um, nodes))
+    pts = np.stack(np.meshgrid(ticks, ticks, indexing="ij"), -1).reshape(-1, 2)
+    out = np.empty((len(depths_um), nodes, nodes, kx, ky, kz))
+    for k, d in enumerate(depths_um):
+        cfg = cls(volume_um=(fov_um, fov_um, 16.0), vres=1.0, ss=1, depth_um=base_depth_um + float(d),
+                  psf_um=(float(kx + 1), float(ky + 1), float(kz)), prop_um=5.0, tail_um=20.0, propcrop=False)
+        raw = raw_fields(cfg, field_shapes(cfg), sigma=sigma, rms=rms, seed=seed + k)
+        psf = run_stage(cfg, raw, pts, device=device, tails=False)["psf_3d"]
+        out[k] = np.maximum(psf[:, 1:, 1:, :kz], 0.0).reshape(nodes, nodes, kx, ky, kz)
+    return out, ticks, np.asarray(depths_um, float)

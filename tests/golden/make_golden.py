@@ -318,9 +318,26 @@ def make_fields(torch):
     return res
 
 
+def make_rana_files(torch):
+    """Files written by the reference's own FullFieldPSF.save / DepthPSFBank.save
+    (maomi/rana/fields.py:96-110, depth.py:50-69) for the format round trips.
+    Writes ref_full_field_psf.npz and ref_depth_psf_bank.npz next to this
+    script; returns the inputs that built them."""
+    from maomi.rana import DepthPSFBank, FullFieldPSF
+    rng = np.random.default_rng(808)
+    k = rng.uniform(0.1, 1.0, (2, 3, 5, 4, 3))
+    x, y = np.array([0.0, 7.5]), np.array([-2.0, 1.0, 6.0])
+    f = FullFieldPSF(k, x, y, (0.5, 0.5, 1.0), 920.0, "excitation", {"note": "reference-written", "n": 3})
+    f.save(HERE / "ref_full_field_psf.npz")
+    ks = rng.uniform(0.1, 1.0, (2, 2, 3, 5, 4, 3))
+    fields = tuple(FullFieldPSF(ks[i], x, y, (0.5, 0.5, 1.0), 920.0, "detection", {"depth": i}) for i in range(2))
+    DepthPSFBank(np.array([1.0, 9.0]), fields).save(HERE / "ref_depth_psf_bank.npz")
+    return {"field_kernels": k, "bank_kernels": ks, "x_um": x, "y_um": y}
+
+
 MAKERS = (("numerics", make_numerics), ("local_fft", make_local_fft), ("stage_small", make_stage_small),
           ("stage_reftest", make_stage_reftest), ("stage_bench_sites", make_stage_bench_sites),
-          ("fields", make_fields), ("stage_bench_lattice", make_stage_bench_lattice))
+          ("fields", make_fields), ("stage_bench_lattice", make_stage_bench_lattice), ("rana_files", make_rana_files))
 
 
 def main(ref_path, only=None):

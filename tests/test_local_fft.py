@@ -74,3 +74,52 @@ def test_cuda_operator_large_kernels_vs_oracle():
         got = RanaOperator(DepthPSFBank(depths, fields), device="cuda").static(vol)
         ref = L.static([kern[0], kern[1]], xs, ys, (1., 1., 1.), vol, operator=op, depths=depths)
         assert rel_l2(got, ref) < RTOL, op
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("xs,ys", [(np.array([0., 1.5, 2.0, 9.0, 40.0]), np.linspace(0, 36, 7)),
+                                   (np.linspace(0, 40, 3), np.array([0., 3., 4., 30., 36.]))])
+def test_cuda_operator_uneven_and_dense_nodes(xs, ys):
+    """Irregular node grids: intervals from 0.5 to 31 pixels (tiles split to
+    <= 18 pixels, one-pixel tiles, single-node pixels), 9x7x5 kernels with
+    even and odd extents, every operator mode, static and scan slabs."""
+    from maomi_b200.rana import DepthPSFBank, FullFieldPSF, RanaOperator
+    rng = np.random.default_rng(17)
+    vol = rng.uniform(0, 1, (40, 36, 7))
+    kern = rng.uniform(0.05, 1, (2, len(xs), len(ys), 9, 6, 5))
+    depths = np.array([0.0, 7.0])
+    for op in ("excitation", "detection"):
+        fields = tuple(FullFieldPSF(kern[i], xs, ys, (1., 1., 1.), 920., op) for i in range(2))
+        for native in (False, True):
+            R = RanaOperator(DepthPSFBank(depths, fields), native=native, device="cuda")
+            ref = L.static([kern[0], kern[1]], xs, ys, (1., 1., 1.), vol, operator=op, depths=depths, native=native)
+            assert rel_l2(R.static(vol), ref) < RTOL, (op, native)
+            for avg in (1, 2):
+                got = R.scan_slab(vol[..., 1:6], z_start=1, scan_avg=avg)
+                ref = L.scan_slab([kern[0], kern[1]], xs, ys, (1., 1., 1.), vol[..., 1:6], operator=op,
+                                  depths=depths, z_start=1, native=native, scan_avg=avg)
+                assert rel_l2(got, ref) < RTOL, (op, native, avg)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("plane", [False, True])
+@pytest.mark.parametrize("detection,correlate", [(False, True), (False, False), (True, False)])
+def test_local_fft_plan_drop_in(plane, detection, correlate):
+    """LocalFFTPlan called directly (the reference's plan API) against the
+    oracle's restatement of the same plan."""
+    from maomi_b200.rana import LocalFFTPlan
+    from maomi_b200.rana.operator import _axis_weights
+    rng = np.random.default_rng(5)
+    shape = (30, 26, 5)
+    kern = rng.uniform(0.1, 1, (3, 4, 7, 5, 5))
+    w = (_axis_weights(np.linspace(0, 30, 3), np.arange(30) + .5),
+         _axis_weights(np.linspace(0, 26, 4), np.arange(26) + .5))
+    src = rng.uniform(0, 1, shape)
+    plan = LocalFFTPlan(shape, kern, w, plane=plane, detection=detection, correlate=correlate, device="cuda")
+    got = plan(src).cpu().numpy()
+    again = plan(src).cpu().numpy()
+    ref = L.local_fft(shape, kern, w, src, plane=plane, detection=detection, correlate=correlate)
+    assert got.shape == ref.shape
+    assert rel_l2(got, ref) < RTOL
+    np.testing.assert_array_equal(again, got)
+    assert plan.stats == {"kernel_fft_builds": 0, "cache_hits": 1} and plan.cache_bytes == 0
