@@ -82,9 +82,22 @@ struct Common {
 
 __device__ __forceinline__ double wz_at(const Common& c, int f, int z) { return c.wz ? c.wz[(size_t)f * c.sz + z] : 1.0; }
 
-__device__ __forceinline__ double kernel_tap(const Common& c, const double* kij, int ux, int uy, int kp) {
-  const int fx = c.flip ? c.kx - 1 - ux : ux, fy = c.flip ? c.ky - 1 - uy : uy;
-  return kij[((size_t)fx * c.ky + fy) * c.kz + kp];
+
+// Kernels re-laid for staging: (nf, nx, ny, kz, kx, ky), already flipped for
+// convolutions (x and y always, z only in 3-D mode), so one kernel plane of
+// one node pair is a contiguous run of kx*ky values.
+__global__ void kernel_prep_kernel(const double* __restrict__ k, int n_pairs, int kx, int ky, int kz, int flip,
+                                   int plane, double* __restrict__ kt) {
+  const size_t per = (size_t)kx * ky * kz;
+  const size_t total = per * n_pairs;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
+    const size_t pair = e / per;
+    const int r = int(e % per);
+    const int kp = r / (kx * ky), uv = r % (kx * ky), ux = uv / ky, uy = uv % ky;
+    const int fx = flip ? kx - 1 - ux : ux, fy = flip ? ky - 1 - uy : uy;
+    const int fz = (flip && !plane) ? kz - 1 - kp : kp;
+    kt[e] = k[pair * per + ((size_t)fx * ky + fy) * kz + fz];
+  }
 }
 
 // ---------------------------------------------------- cell kernel (gather)
@@ -99,12 +112,64 @@ static_assert(TMAX * CH <= GROUP, "one unit per thread");
 
 struct CellP {
   Common c;
-  const int* tx;   // x tiles (kTileInts each)
+  const double* kt;  // kernel_prep_kernel layout
+  const int* tx;     // x tiles (kTileInts each)
   const int* ty;
   int ntx, nty;
-  int hx, hy;      // halo plane extents (hy padded against bank conflicts)
-  int kplanes;     // kernel-plane slots in shared memory (1, or TZC in plane mode)
+  int hx, hy;        // halo plane extents (hy padded against bank conflicts)
+  int kplanes;       // kernel-plane slots in shared memory (1, or TZC in plane mode)
 };
+
+// One halo row of taps for NP node pairs: acc[p][q] += sum_uy h[q + uy] k_p[uy].
+// The window w slides along y in chunks of QY taps; the chunk loop has no
+// data-dependent branches (the remainder of ky is a separate tail).
+template <int NP>
+__device__ __forceinline__ void taps_row(const double* __restrict__ hrow, const double* __restrict__ krow, int kplane,
+                                         int ky, double (&acc)[PG][QY]) {
+  double w[2 * QY];
+#pragma unroll
+  for (int q = 0; q < QY; ++q) w[q] = hrow[q];
+  const int nfull = ky / QY;
+#pragma unroll 1
+  for (int cidx = 0; cidx < nfull; ++cidx) {
+    const int uy0 = cidx * QY;
+#pragma unroll
+    for (int q = 0; q < QY; ++q) w[QY + q] = hrow[uy0 + QY + q];
+#pragma unroll
+    for (int ph = 0; ph < QY; ++ph)
+#pragma unroll
+      for (int p = 0; p < NP; ++p) {
+        const double kv = krow[p * kplane + uy0 + ph];
+#pragma unroll
+        for (int q = 0; q < QY; ++q) acc[p][q] = fma(w[q + ph], kv, acc[p][q]);
+      }
+#pragma unroll
+    for (int q = 0; q < QY; ++q) w[q] = w[QY + q];
+  }
+  const int rem = ky - nfull * QY;
+  if (rem > 0) {
+    const int uy0 = nfull * QY;
+#pragma unroll
+    for (int q = 0; q < QY; ++q) w[QY + q] = hrow[uy0 + QY + q];
+#pragma unroll
+    for (int ph = 0; ph < QY; ++ph)
+      if (ph < rem)
+#pragma unroll
+        for (int p = 0; p < NP; ++p) {
+          const double kv = krow[p * kplane + uy0 + ph];
+#pragma unroll
+          for (int q = 0; q < QY; ++q) acc[p][q] = fma(w[q + ph], kv, acc[p][q]);
+        }
+  }
+}
+
+template <int NP>
+__device__ __forceinline__ void taps_plane(const double* hbase, const double* kbase, int hy, int kx, int ky,
+                                           double (&acc)[PG][QY]) {
+  const int kplane = kx * ky;
+#pragma unroll 1
+  for (int ux = 0; ux < kx; ++ux) taps_row<NP>(hbase + (size_t)ux * hy, kbase + (size_t)ux * ky, kplane, ky, acc);
+}
 
 __global__ void __launch_bounds__(CELL_THREADS, 2) cell_kernel(CellP P) {
   extern __shared__ double smem[];
@@ -122,6 +187,7 @@ __global__ void __launch_bounds__(CELL_THREADS, 2) cell_kernel(CellP P) {
   }
   if (!ok) return;  // uniform per CTA
   const int tid = threadIdx.x;
+  const int warp = tid / 32, lane = tid % 32;
   const int g = tid / GROUP;                 // plane group
   const int u = tid % GROUP;
   const int ch = u / TMAX, row = u % TMAX;   // rows fastest: conflict-free halo reads
@@ -131,9 +197,10 @@ __global__ void __launch_bounds__(CELL_THREADS, 2) cell_kernel(CellP P) {
   const int hplane = P.hx * P.hy;
   const int kplane = c.kx * c.ky;
   double* halo = smem;                                         // [TZC][hx][hy]
-  double* ks = smem + (size_t)TZC * hplane;                    // [kplanes][PG][kx][ky]
+  double* ks = smem + (size_t)TZC * hplane;                    // [kplanes][PG][kx*ky]
   const int npairs = ax * ay;
   const int iters = c.plane ? (c.kz + TZC - 1) / TZC : c.kz;
+  const size_t pair_stride = (size_t)c.kz * kplane;
 
   double fin[QY];
 #pragma unroll
@@ -148,7 +215,7 @@ __global__ void __launch_bounds__(CELL_THREADS, 2) cell_kernel(CellP P) {
     }
     const double wzo = (!c.plane && oz < c.sz) ? wz_at(c, f, oz) : 1.0;
     const bool live = unit && (c.plane || (oz < c.sz && wzo != 0.0));
-    const double* kf = c.kern + (size_t)f * c.nx * c.ny * kplane * c.kz;
+    const double* kf = P.kt + (size_t)f * c.nx * c.ny * pair_stride;
     for (int p0 = 0; p0 < npairs; p0 += PG) {
       const int np = min(PG, npairs - p0);
       double acc[PG][QY];
@@ -157,61 +224,48 @@ __global__ void __launch_bounds__(CELL_THREADS, 2) cell_kernel(CellP P) {
 #pragma unroll
         for (int q = 0; q < QY; ++q) acc[p][q] = 0.0;
       for (int it = 0; it < iters; ++it) {
-        __syncthreads();
-        // ---- source halo: plane for each group (zero outside the volume)
-        for (int e = tid; e < TZC * hplane; e += CELL_THREADS) {
-          const int gg = e / hplane, rem = e % hplane, hxi = rem / P.hy, hyi = rem % P.hy;
-          int gz;
-          if (c.plane) gz = it * TZC + gg;
-          else gz = z0 + gg + it - c.cz;
-          const int gx = x0 - c.cx + hxi, gy = y0 - c.cy + hyi;
-          double v = 0.0;
-          if (gx >= 0 && gx < c.sx && gy >= 0 && gy < c.sy && gz >= 0 && gz < c.sz && (c.plane ? gz < c.kz : true))
-            v = c.srcT[((size_t)gz * c.sx + gx) * c.sy + gy];
-          halo[e] = v;
+        __syncthreads();  // the previous iteration's readers are done
+        // ---- source halo planes, rows per warp, y across lanes (zero fill
+        // outside the volume); all copies of the iteration in flight at once
+        for (int gg = 0; gg < TZC; ++gg) {
+          const int gz = c.plane ? it * TZC + gg : z0 + gg + it - c.cz;
+          const bool zin = gz >= 0 && gz < c.sz;
+          const double* splane = c.srcT + (size_t)(zin ? gz : 0) * c.sx * c.sy;
+          for (int hxi = warp; hxi < P.hx; hxi += CELL_THREADS / 32) {
+            const int gx = x0 - c.cx + hxi;
+            const bool xin = zin && gx >= 0 && gx < c.sx;
+            const double* srow = splane + (size_t)(xin ? gx : 0) * c.sy;
+            double* drow = halo + (size_t)gg * hplane + (size_t)hxi * P.hy;
+            for (int hyi = lane; hyi < P.hy; hyi += 32) {
+              const int gy = y0 - c.cy + hyi;
+              const bool in = xin && gy >= 0 && gy < c.sy;
+              cp_async8_zfill(drow + hyi, srow + (in ? gy : 0), in);
+            }
+          }
         }
-        // ---- kernel planes of this pass's pairs (flipped for convolutions)
-        for (int e = tid; e < P.kplanes * np * kplane; e += CELL_THREADS) {
-          const int slot = e / (np * kplane), rem = e % (np * kplane), p = rem / kplane, uv = rem % kplane;
-          const int ux = uv / c.ky, uy = uv % c.ky;
-          const int pair = p0 + p, i = tx[3 + pair / ay], j = ty[3 + pair % ay];
-          const double* kij = kf + ((size_t)i * c.ny + j) * kplane * c.kz;
-          int kp;
-          if (c.plane) kp = it * TZC + slot;
-          else kp = c.flip ? c.kz - 1 - it : it;
-          ks[((size_t)slot * PG + p) * kplane + uv] = kp < c.kz ? kernel_tap(c, kij, ux, uy, kp) : 0.0;
+        // ---- this pass's kernel planes: contiguous runs of kx*ky values
+        for (int slot = 0; slot < P.kplanes; ++slot) {
+          const int kp = c.plane ? it * TZC + slot : it;
+          for (int p = 0; p < np; ++p) {
+            const int pair = p0 + p, i = tx[3 + pair / ay], j = ty[3 + pair % ay];
+            const bool kin = kp < c.kz;
+            const double* src = kf + ((size_t)i * c.ny + j) * pair_stride + (size_t)(kin ? kp : 0) * kplane;
+            double* dst = ks + ((size_t)slot * PG + p) * kplane;
+            for (int e = tid; e < kplane; e += CELL_THREADS) cp_async8_zfill(dst + e, src + e, kin);
+          }
         }
+        cp_async_commit();
+        cp_async_wait_all();
         __syncthreads();
         if (!live) continue;
         if (c.plane && it * TZC + g >= c.kz) continue;
         const double* hbase = halo + (size_t)g * hplane + (size_t)row * P.hy + ch * QY;
         const double* kbase = ks + (size_t)(c.plane ? g : 0) * PG * kplane;
-        for (int ux = 0; ux < c.kx; ++ux) {
-          const double* hrow = hbase + (size_t)ux * P.hy;
-          const double* krow = kbase + (size_t)ux * c.ky;
-          double w[2 * QY];
-#pragma unroll
-          for (int q = 0; q < QY; ++q) w[q] = hrow[q];
-          for (int uy0 = 0; uy0 < c.ky; uy0 += QY) {
-#pragma unroll
-            for (int q = 0; q < QY; ++q) w[QY + q] = hrow[uy0 + QY + q];
-            const int nph = min(QY, c.ky - uy0);
-#pragma unroll
-            for (int ph = 0; ph < QY; ++ph) {
-              if (ph < nph) {
-#pragma unroll
-                for (int p = 0; p < PG; ++p) {
-                  if (p < np) {
-                    const double kv = krow[(size_t)p * kplane + uy0 + ph];
-#pragma unroll
-                    for (int q = 0; q < QY; ++q) acc[p][q] = fma(w[q + ph], kv, acc[p][q]);
-                  }
-                }
-              }
-            }
-#pragma unroll
-            for (int q = 0; q < QY; ++q) w[q] = w[QY + q];
-          }
+        switch (np) {
+          case 4: taps_plane<4>(hbase, kbase, P.hy, c.kx, c.ky, acc); break;
+          case 3: taps_plane<3>(hbase, kbase, P.hy, c.kx, c.ky, acc); break;
+          case 2: taps_plane<2>(hbase, kbase, P.hy, c.kx, c.ky, acc); break;
+          default: taps_plane<1>(hbase, kbase, P.hy, c.kx, c.ky, acc); break;
         }
       }
       // ---- fold the pairs with their pixel weights
@@ -266,6 +320,7 @@ constexpr int GEN_THREADS = TX * (TY / GQY) * TZ;  // 128
 
 struct GenP {
   Common c;
+  const double* kt;  // kernel_prep_kernel layout
   int kyp;         // ky padded to a multiple of GQY
   int hx, hy;
   int detection;
@@ -321,7 +376,7 @@ __global__ void __launch_bounds__(GEN_THREADS) generic_kernel(GenP P) {
       }
       if (!any) continue;
     }
-    const double* kf = c.kern + (size_t)f * c.nx * c.ny * c.kx * c.ky * c.kz;
+    const double* kf = P.kt + (size_t)f * c.nx * c.ny * c.kx * c.ky * c.kz;
     for (int i = 0; i < c.nx; ++i) {
       const bool ai = P.detection ? touches(lox[i], hix[i], sx_lo, sx_hi) : touches(lox[i], hix[i], x0, x0 + TX);
       if (!ai) continue;
@@ -345,10 +400,10 @@ __global__ void __launch_bounds__(GEN_THREADS) generic_kernel(GenP P) {
             }
             halo[e] = v;
           }
+          const double* kpl = kij + (size_t)dz * c.kx * c.ky;  // prepped: flips applied
           for (int e = tid; e < c.kx * P.kyp; e += GEN_THREADS) {
             const int ux = e / P.kyp, uy = e % P.kyp;
-            const int kp = (c.flip && !c.plane) ? c.kz - 1 - dz : dz;
-            ks[e] = uy < c.ky ? kernel_tap(c, kij, ux, uy, kp) : 0.0;
+            ks[e] = uy < c.ky ? kpl[(size_t)ux * c.ky + uy] : 0.0;
           }
           __syncthreads();
           if (tzi < nzo) {
@@ -485,9 +540,21 @@ extern "C" int mm_local_tiles(const double* w, int nodes, int n, int max_len, in
   return ntiles;
 }
 
+namespace mm {
+namespace {
+size_t round256(size_t b) { return (b + 255) / 256 * 256; }
+size_t source_bytes(const mm_local_desc* d) { return round256((size_t)d->sx * d->sy * d->sz * sizeof(double)); }
+size_t kernel_bytes(const mm_local_desc* d) {
+  return round256((size_t)d->nfields * d->nodes_x * d->nodes_y * d->kx * d->ky * d->kz * sizeof(double));
+}
+}  // namespace
+}  // namespace mm
+
 extern "C" size_t mm_local_render_workspace_size(const mm_local_desc* d) {
-  if (!d || d->sx < 1 || d->sy < 1 || d->sz < 1) return 0;
-  return ((size_t)d->sx * d->sy * d->sz * sizeof(double) + 255) / 256 * 256;
+  if (!d || d->sx < 1 || d->sy < 1 || d->sz < 1 || d->kx < 1 || d->ky < 1 || d->kz < 1 || d->nodes_x < 1 ||
+      d->nodes_y < 1 || d->nfields < 1)
+    return 0;
+  return mm::source_bytes(d) + mm::kernel_bytes(d);
 }
 
 extern "C" int mm_local_render(const mm_local_desc* d, const double* source, const double* zweight, double* out,
@@ -504,17 +571,23 @@ extern "C" int mm_local_render(const mm_local_desc* d, const double* source, con
   const size_t need = mm_local_render_workspace_size(d);
   MM_CHECK_ARG(workspace && workspace_bytes >= need, "workspace too small: %zu bytes given, %zu needed",
                workspace_bytes, need);
+  MM_CHECK_ARG(reinterpret_cast<uintptr_t>(workspace) % 256 == 0, "workspace must be 256-byte aligned");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   double* srcT = static_cast<double*>(workspace);
+  double* kt = reinterpret_cast<double*>(static_cast<char*>(workspace) + source_bytes(d));
   transpose_kernel<<<dim3(d->sx, (d->sy + 31) / 32), 256, 0, s>>>(source, d->sx, d->sy, d->sz, srcT);
   MM_CHECK_LAUNCH("local render transpose");
   const Common c = common_params(d, srcT, zweight, out);
+  kernel_prep_kernel<<<1184, 256, 0, s>>>(d->kernels, d->nfields * d->nodes_x * d->nodes_y, d->kx, d->ky, d->kz,
+                                          c.flip, c.plane, kt);
+  MM_CHECK_LAUNCH("local render kernel layout");
   if (!d->detection) {
     MM_CHECK_ARG(d->tiles_x && d->tiles_y && d->ntiles_x >= 0 && d->ntiles_y >= 0,
                  "excitation/native render needs the mm_local_tiles tables");
     if (d->ntiles_x == 0 || d->ntiles_y == 0) return MM_OK;  // no active node anywhere
     CellP P{};
     P.c = c;
+    P.kt = kt;
     P.tx = d->tiles_x;
     P.ty = d->tiles_y;
     P.ntx = d->ntiles_x;
@@ -538,6 +611,7 @@ extern "C" int mm_local_render(const mm_local_desc* d, const double* source, con
   }
   GenP P{};
   P.c = c;
+  P.kt = kt;
   P.detection = d->detection;
   P.kyp = (d->ky + GQY - 1) / GQY * GQY;
   P.hx = TX + d->kx - 1;
