@@ -309,6 +309,8 @@ int mm_propagate_items(const mm_item_class* c, void* workspace, size_t workspace
  * psf_abs_sum are given, the site sums of psf and |psf| (FP64).  Replaces the
  * focal ResamplePlan call of maomi/backends/cuda/batched.py:194-200 and the
  * reductions of maomi/fixed.py:126,153-154.  psf may be NULL (energies only).
+ * All four tables NULL: identity resample (ss = 1; X == H, Y == W), run as a
+ * tiled transpose of the crops.
  */
 int mm_focal_finalize(const float* focal /* (P,Z,H,W) */, const int32_t* ix, const float* wx, int KX,
                       const int32_t* iy, const float* wy, int KY, const float* axial /* (Z) */, float scale,
@@ -494,6 +496,82 @@ int mm_surrogate_inputs(const float* const* raw, const int* zpart, int h, int w,
                         void* stream);
 /* y (S,4096,16) -> PSF planes (S,9,64,64), negatives clipped to 0. */
 int mm_surrogate_planes(const float* y, float* out, int sites, void* stream);
+
+/* ------------------------------------------------------------------------
+ * Static and per-frame scan operators: 2-D linear convolutions of real
+ * planes with real kernel planes through zero-padded 2-D DFTs (sizes
+ * fx x fy, powers of two 64..1024) and a per-bin coupling rule along Z.
+ *
+ * Replaces:
+ *   zstack                 maomi/scanning.py:8-53   (CONV_Z / CORR_Z rules)
+ *   psf_fft, _group_z      maomi/movie.py:32-42     (mm_scan_kernel_spectrum)
+ *   single_scan            maomi/movie.py:48-66     (SUM_Z rule)
+ *   blurred_background     maomi/movie.py:69-102    (mm_scan_background + EACH_Z)
+ *   conv2_same             maomi/movie.py:14-19     (EACH_Z, one plane)
+ *
+ * Data are float32 (fp64 = 0, FP32 transforms) or float64 (fp64 = 1, FP64
+ * transforms).  Planes are addressed through element strides, so slabs of a
+ * larger (X, Y, Z) array need no copy.  Transform planes are packed two to
+ * a complex transform; spectra stay on the device.
+ * ------------------------------------------------------------------------ */
+enum {
+  MM_SCAN_CONV_Z = 0, /* out[o] = sum_l src[o + zoff - l] * k[l]  (3-D convolution, zero extended)   */
+  MM_SCAN_CORR_Z = 1, /* out[o] = sum_l src[o - zoff + l] * k[l]  (correlation along Z, zero extended) */
+  MM_SCAN_SUM_Z = 2,  /* out[0] = sum_z src[z] * k[z]              (one frame: sum of plane convolutions) */
+  MM_SCAN_EACH_Z = 3  /* out[z] = src[z] * k[z]                    (independent planes) */
+};
+
+typedef struct {
+  const void* data;       /* element (x, y, z) at data[x*s0 + y*s1 + z*s2] */
+  long long s0, s1, s2;   /* element strides */
+  int nx, ny, nz;         /* extents */
+  int group;              /* consecutive planes summed into one transform plane (scan_avg); >= 1 */
+  const void* mask0;      /* optional nx*ny row-major multipliers of every plane (NULL: none) */
+  const void* mask1;
+} mm_scan_planes;
+
+typedef struct {
+  int fp64;               /* 0: float32 data / FP32 transforms; 1: float64 / FP64 */
+  int fx, fy;             /* transform sizes: powers of two in 64..1024 */
+  int kx, ky;             /* kernel plane extents */
+  int kplanes;            /* kernel transform planes (after grouping) */
+} mm_scan_desc;
+
+typedef struct {
+  mm_scan_planes src;
+  int wrap;               /* 1: periodic extension: transform input row i = source row (i + wrap_x0) mod nx */
+  int wrap_x0, wrap_y0;
+  int ext_x, ext_y;       /* nonzero transform-input rows / columns (nx, ny without wrap) */
+  int zrule;              /* MM_SCAN_* */
+  int zoff;               /* Z offset of the CONV / CORR rules (kernel planes / 2) */
+  int out_planes;         /* output planes (1 for SUM_Z) */
+  int crop_x, crop_y;     /* first kept row / column of the linear convolution */
+  int out_x, out_y;       /* kept rows / columns */
+  void* out;              /* element (x, y, o) at out[x*o0 + y*o1 + o*o2], data type of the call */
+  long long o0, o1, o2;
+  int accumulate;         /* 1: out += alpha * result; 0: out = alpha * result */
+  double alpha;
+} mm_scan_conv;
+
+/* Bytes of a kernel spectrum (kplanes half spectra fx x (fy/2+1), complex). */
+size_t mm_scan_spectrum_bytes(const mm_scan_desc* desc);
+/* Bytes of workspace for `planes` transform planes (packed complex spectra). */
+size_t mm_scan_workspace_size(const mm_scan_desc* desc, int planes);
+/* Spectra of the (grouped) kernel planes into `spectrum` (psf_fft). */
+int mm_scan_kernel_spectrum(const mm_scan_desc* desc, const mm_scan_planes* kernel, void* spectrum,
+                            void* workspace, size_t workspace_bytes, void* stream);
+/* One convolution pass: forward DFT of the (grouped, masked, optionally
+ * wrapped) source planes, the Z rule against `spectrum`, inverse DFT, crop,
+ * scale and store or accumulate. */
+int mm_scan_convolve(const mm_scan_desc* desc, const mm_scan_conv* conv, const void* spectrum, void* workspace,
+                     size_t workspace_bytes, void* stream);
+/* The background source plane of blurred_background (movie.py:86-95):
+ * out[x,y] = power * mask[x,y] / n * sum_i scale[i] * sum_v vol_v[x,y,idx[i]]
+ * over nvol volumes that share one layout (s0, s1, s2); mask may be NULL.
+ * idx: (n) int32 device array; scale: (n) float64 device array. */
+int mm_scan_background(int fp64, const void* const* volumes, int nvol, long long s0, long long s1, long long s2,
+                       int nx, int ny, int nz, const int32_t* idx, const double* scale, int n, double power,
+                       const void* mask, void* out, void* stream);
 
 #ifdef __cplusplus
 }

@@ -65,6 +65,26 @@ class LocalDesc(Structure):
                 ("tiles_x", c_void_p), ("ntiles_x", c_int), ("tiles_y", c_void_p), ("ntiles_y", c_int)]
 
 
+class ScanPlanes(Structure):
+    _fields_ = [("data", c_void_p), ("s0", ctypes.c_longlong), ("s1", ctypes.c_longlong), ("s2", ctypes.c_longlong),
+                ("nx", c_int), ("ny", c_int), ("nz", c_int), ("group", c_int), ("mask0", c_void_p),
+                ("mask1", c_void_p)]
+
+
+class ScanDesc(Structure):
+    _fields_ = [("fp64", c_int), ("fx", c_int), ("fy", c_int), ("kx", c_int), ("ky", c_int), ("kplanes", c_int)]
+
+
+class ScanConv(Structure):
+    _fields_ = [("src", ScanPlanes), ("wrap", c_int), ("wrap_x0", c_int), ("wrap_y0", c_int), ("ext_x", c_int),
+                ("ext_y", c_int), ("zrule", c_int), ("zoff", c_int), ("out_planes", c_int), ("crop_x", c_int),
+                ("crop_y", c_int), ("out_x", c_int), ("out_y", c_int), ("out", c_void_p), ("o0", ctypes.c_longlong),
+                ("o1", ctypes.c_longlong), ("o2", ctypes.c_longlong), ("accumulate", c_int), ("alpha", c_double)]
+
+
+MM_SCAN_CONV_Z, MM_SCAN_CORR_Z, MM_SCAN_SUM_Z, MM_SCAN_EACH_Z = 0, 1, 2, 3
+
+
 class SurrogateDesc(ctypes.Structure):
     _fields_ = [("sites", c_int), ("F", c_void_p), ("G", c_void_p), ("FT", c_void_p),
                 ("GT", c_void_p), ("params", c_void_p), ("grads", c_void_p),
@@ -130,6 +150,14 @@ SIGNATURES = {
     "mm_local_tiles": (c_int, [c_void_p, c_int, c_int, c_int, c_void_p, c_int]),
     "mm_local_render_workspace_size": (c_size_t, [POINTER(LocalDesc)]),
     "mm_local_render": (c_int, [POINTER(LocalDesc), c_void_p, c_void_p, c_void_p, c_void_p, c_size_t, c_void_p]),
+    "mm_scan_spectrum_bytes": (c_size_t, [POINTER(ScanDesc)]),
+    "mm_scan_workspace_size": (c_size_t, [POINTER(ScanDesc), c_int]),
+    "mm_scan_kernel_spectrum": (c_int, [POINTER(ScanDesc), POINTER(ScanPlanes), c_void_p, c_void_p, c_size_t,
+                                        c_void_p]),
+    "mm_scan_convolve": (c_int, [POINTER(ScanDesc), POINTER(ScanConv), c_void_p, c_void_p, c_size_t, c_void_p]),
+    "mm_scan_background": (c_int, [c_int, POINTER(c_void_p), c_int, ctypes.c_longlong, ctypes.c_longlong,
+                                   ctypes.c_longlong, c_int, c_int, c_int, c_void_p, c_void_p, c_int, c_double,
+                                   c_void_p, c_void_p, c_void_p]),
 }
 
 _lib = None

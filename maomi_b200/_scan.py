@@ -1,0 +1,128 @@
+"""Host side of the plane-convolution engine (``csrc/scan.cu``) shared by
+``maomi_b200.scanning`` (zstack) and ``maomi_b200.movie`` (single_scan,
+blurred_background, conv2_same, psf_fft).
+
+Every operator here is a linear 2-D convolution of real planes with real
+kernel planes, evaluated through zero-padded DFTs of power-of-two sizes and
+cropped to the window the reference keeps.  The transform size of an axis
+only has to keep that window alias free: for a source of extent ``e``, a
+kernel of extent ``k`` and a first kept index ``c`` the linear convolution
+ends at ``e + k - 1``, so ``f >= max(c + out, e + k - 1 - c)``.
+"""
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+
+MIN_SIZE, MAX_SIZE = 64, 1024
+
+
+def transform_size(need):
+    """Smallest supported power of two >= ``need``."""
+    n = MIN_SIZE
+    while n < need:
+        n *= 2
+    if n > MAX_SIZE:
+        raise ValueError(f"plane convolution needs a transform of {need} samples; this build supports up to "
+                         f"{MAX_SIZE} (volumes up to about {MAX_SIZE} pixels across with small kernels)")
+    return n
+
+
+def real_dtype(t):
+    """float32 and float64 planes are convolved in their own precision."""
+    import torch
+    if t.dtype == torch.float64:
+        return 1
+    if t.dtype == torch.float32:
+        return 0
+    raise ValueError(f"plane convolution supports float32 and float64 data, got {t.dtype}")
+
+
+def planes_record(t, *, group=1, masks=(None, None)):
+    """ScanPlanes of a 3-D device tensor (any strides), optional XY masks."""
+    s = t.stride()
+    m0, m1 = masks
+    return _lib.ScanPlanes(t.data_ptr(), s[0], s[1], s[2], t.shape[0], t.shape[1], t.shape[2], int(group),
+                           None if m0 is None else m0.data_ptr(), None if m1 is None else m1.data_ptr())
+
+
+class KernelSpectrum:
+    """Device half spectra of (grouped) kernel planes at one transform size.
+
+    ``fx``, ``fy``: transform sizes; ``kx``, ``ky``: kernel plane extents;
+    ``planes``: kernel transform planes (after grouping); ``fp64``."""
+
+    def __init__(self, kernel, fx, fy, *, group=1):
+        import torch
+        self.device = kernel.device
+        self.fp64 = real_dtype(kernel)
+        self.dtype = kernel.dtype
+        self.fx, self.fy = int(fx), int(fy)
+        self.kx, self.ky = int(kernel.shape[0]), int(kernel.shape[1])
+        self.group = int(group)
+        self.planes = -(-int(kernel.shape[2]) // self.group)
+        self.desc = _lib.ScanDesc(self.fp64, self.fx, self.fy, self.kx, self.ky, self.planes)
+        lib = _lib.load()
+        nbytes = lib.mm_scan_spectrum_bytes(ctypes.byref(self.desc))
+        if nbytes == 0:
+            _lib.check(_lib.MM_ERR_UNSUPPORTED, _lib.last_error() or "scan descriptor rejected")
+        self.data = torch.empty(nbytes, dtype=torch.uint8, device=self.device)
+        work = workspace(self.desc, self.planes, self.device)
+        rec = planes_record(kernel, group=self.group)
+        _lib.check(lib.mm_scan_kernel_spectrum(ctypes.byref(self.desc), ctypes.byref(rec), _lib.ptr(self.data),
+                                               _lib.ptr(work), work.numel(), _lib.stream_of(self.device)),
+                   "kernel spectrum")
+        self._keep = kernel  # the kernel stays alive until the stream has read it
+
+    def convolve(self, src, *, zrule, out, crop, out_shape, out_planes, zoff=0, group=1, masks=(None, None),
+                 wrap=None, accumulate=False, alpha=1.0):
+        """One engine pass of ``src`` (3-D device tensor) into ``out``."""
+        lib = _lib.load()
+        if src.dtype != self.dtype or out.dtype != self.dtype:
+            raise ValueError("source, kernel and output must share one floating type")
+        rec = planes_record(src, group=group, masks=masks)
+        nin = -(-int(src.shape[2]) // int(group))
+        if wrap is None:
+            wrap_flag, wx0, wy0, ext_x, ext_y = 0, 0, 0, int(src.shape[0]), int(src.shape[1])
+        else:
+            wrap_flag, (wx0, wy0), (ext_x, ext_y) = 1, wrap[0], wrap[1]
+        o = out.stride() if out.dim() == 3 else (out.stride(0), out.stride(1), 0)
+        conv = _lib.ScanConv(rec, wrap_flag, int(wx0), int(wy0), int(ext_x), int(ext_y), int(zrule), int(zoff),
+                             int(out_planes), int(crop[0]), int(crop[1]), int(out_shape[0]), int(out_shape[1]),
+                             out.data_ptr(), o[0], o[1], o[2], int(bool(accumulate)), float(alpha))
+        work = workspace(self.desc, max(nin, int(out_planes)), self.device)
+        _lib.check(lib.mm_scan_convolve(ctypes.byref(self.desc), ctypes.byref(conv), _lib.ptr(self.data),
+                                        _lib.ptr(work), work.numel(), _lib.stream_of(self.device)), "plane convolution")
+        return out
+
+
+def workspace(desc, planes, device):
+    import torch
+    nbytes = _lib.load().mm_scan_workspace_size(ctypes.byref(desc), int(planes))
+    if nbytes == 0:
+        _lib.check(_lib.MM_ERR_UNSUPPORTED, _lib.last_error() or "scan descriptor rejected")
+    return torch.empty(nbytes, dtype=torch.uint8, device=device)
+
+
+def as_device(a, device, dtype=None):
+    """Host or device array -> device tensor (no copy when already there)."""
+    import torch
+    if isinstance(a, torch.Tensor):
+        t = a.to(device=device, dtype=dtype if dtype is not None else a.dtype)
+    else:
+        arr = np.asarray(a)
+        t = _lib.upload(arr, device) if arr.size else torch.as_tensor(arr, device=device)
+        if dtype is not None:
+            t = t.to(dtype)
+    return t
+
+
+def mask_tensor(m, shape, device, dtype):
+    if m is None:
+        return None
+    t = as_device(m, device, dtype)
+    if tuple(t.shape) != tuple(shape):
+        raise ValueError("Mask must match volume XY")
+    return t.contiguous()

@@ -58,6 +58,9 @@ class ResampleTables:
         mx, my = resample_matrix(h, ss), resample_matrix(w, ss)
         (ix, wx), (iy, wy) = sparse_rows(mx), sparse_rows(my)
         self.shape = (mx.shape[0], my.shape[0])
+        #: ss = 1: the resample is the identity (one unit tap per output)
+        self.identity = bool(mx.shape == (h, h) and my.shape == (w, w) and np.array_equal(mx, np.eye(h))
+                             and np.array_equal(my, np.eye(w)))
         self.ix = _lib.upload(ix, device)
         self.wx = _lib.upload(wx, device)
         self.iy = _lib.upload(iy, device)
@@ -266,8 +269,9 @@ class OpticalPlan:
         s1 = torch.empty((X, Y, Z), dtype=torch.float64, device=dev) if sums else None
         s2 = torch.empty((X, Y, Z), dtype=torch.float64, device=dev) if sums else None
         rt = self.focal_resample
-        _lib.call("mm_focal_finalize", _lib.ptr(focal), _lib.ptr(rt.ix), _lib.ptr(rt.wx), rt.ix.shape[1],
-                  _lib.ptr(rt.iy), _lib.ptr(rt.wy), rt.iy.shape[1], _lib.ptr(self.axial_focus),
+        tabs = (None, None, None, None) if rt.identity else (rt.ix, rt.wx, rt.iy, rt.wy)
+        _lib.call("mm_focal_finalize", _lib.ptr(focal), _lib.ptr(tabs[0]), _lib.ptr(tabs[1]), rt.ix.shape[1],
+                  _lib.ptr(tabs[2]), _lib.ptr(tabs[3]), rt.iy.shape[1], _lib.ptr(self.axial_focus),
                   float(np.float32(self.scale)), P, Z, H, W, X, Y, _lib.ptr(out), _lib.ptr(energies),
                   _lib.ptr(s1), _lib.ptr(s2), _lib.stream_of(dev))
         return out, energies, s1, s2

@@ -53,5 +53,8 @@ extern "C" size_t mm_struct_size(const char* name) {
   if (n == "mm_item_class") return sizeof(mm_item_class);
   if (n == "mm_local_desc") return sizeof(mm_local_desc);
   if (n == "mm_surrogate_desc") return sizeof(mm_surrogate_desc);
+  if (n == "mm_scan_planes") return sizeof(mm_scan_planes);
+  if (n == "mm_scan_desc") return sizeof(mm_scan_desc);
+  if (n == "mm_scan_conv") return sizeof(mm_scan_conv);
   return 0;
 }

@@ -88,6 +88,44 @@ __global__ void focal_finalize_kernel(const float* __restrict__ focal, const int
   }
 }
 
+// Identity resample (ss = 1: X = H, Y = W): a tiled transpose of the focal
+// crops (P, Z, X, Y) -> psf (P, X, Y, Z) with the scale and axial weights.
+// grid (ceil(X / kFocalRows), P); both the reads (rows of a plane, y fastest)
+// and the writes (z fastest) are contiguous runs.  Same value expression as
+// focal_finalize_kernel (scale * v * axial[z]).
+constexpr int kFocalRows = 8;
+
+__global__ void focal_transpose_kernel(const float* __restrict__ focal, const float* __restrict__ axial, float scale,
+                                       int Z, int X, int Y, float* __restrict__ psf, double* __restrict__ energies) {
+  extern __shared__ float tile[];  // (rows * Y) x (Z + 1)
+  __shared__ double red[32];
+  const int p = blockIdx.y, x0 = blockIdx.x * kFocalRows;
+  const int rows = min(kFocalRows, X - x0);
+  const int ry = rows * Y;
+  const float* src = focal + (size_t)p * Z * X * Y + (size_t)x0 * Y;
+  double acc = 0.0;
+  for (int e = threadIdx.x; e < Z * ry; e += blockDim.x) {
+    const int z = e / ry, o = e - z * ry;  // o = r * Y + y
+    const float v = scale * __ldg(src + (size_t)z * X * Y + o) * __ldg(axial + z);
+    tile[o * (Z + 1) + z] = v;
+    acc += v;
+  }
+  __syncthreads();
+  if (psf) {
+    float* dst = psf + ((size_t)p * X + x0) * Y * Z;
+    for (int e = threadIdx.x; e < ry * Z; e += blockDim.x) dst[e] = tile[(e / Z) * (Z + 1) + e % Z];
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int w = 0; w < int(blockDim.x >> 5); ++w) s += red[w];
+    atomicAdd(energies + p, s);
+  }
+}
+
 // Partial site sums of psf and |psf|: grid (ceil(E/256), chunks).
 __global__ void site_sums_kernel(const float* __restrict__ psf, long long E, int P, int chunk,
                                  double* __restrict__ sum, double* __restrict__ abs_sum) {
@@ -183,18 +221,33 @@ extern "C" int mm_focal_finalize(const float* focal, const int32_t* ix, const fl
                                  const float* wy, int KY, const float* axial, float scale, int P, int Z, int H, int W,
                                  int X, int Y, float* psf, double* energies, double* psf_sum, double* psf_abs_sum,
                                  void* stream) {
-  MM_CHECK_ARG(focal && ix && wx && iy && wy && axial && energies, "NULL pointer");
+  const bool identity = !ix && !wx && !iy && !wy;
+  MM_CHECK_ARG(focal && axial && energies && (identity || (ix && wx && iy && wy)), "NULL pointer");
   MM_CHECK_ARG(P >= 1 && Z >= 1 && H >= 1 && W >= 1 && X >= 1 && Y >= 1 && P <= 65535, "bad focal sizes");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   MM_CHECK_CUDA(cudaMemsetAsync(energies, 0, sizeof(double) * P, s), "zero energies");
+  if (identity) {
+    MM_CHECK_ARG(X == H && Y == W, "identity focal resample needs X == H and Y == W (got %d x %d from %d x %d)", X, Y,
+                 H, W);
+    const size_t tt = sizeof(float) * (size_t)kFocalRows * Y * (Z + 1);
+    MM_CHECK_ARG(tt <= 200 * 1024, "focal crop %d x %d planes too large for one tile", Y, Z);
+    if (tt > 48 * 1024)
+      MM_CHECK_CUDA(cudaFuncSetAttribute(focal_transpose_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tt),
+                    "cudaFuncSetAttribute(focal transpose)");
+    focal_transpose_kernel<<<dim3((X + kFocalRows - 1) / kFocalRows, P), 256, tt, s>>>(focal, axial, scale, Z, X, Y,
+                                                                                          psf, energies);
+    MM_CHECK_LAUNCH("focal transpose");
+  }
   const size_t tile = sizeof(float) * (size_t)Y * (Z + 1);
   MM_CHECK_ARG(tile <= 200 * 1024, "focal crop %d x %d planes too large for one tile", Y, Z);
-  if (tile > 48 * 1024)
-    MM_CHECK_CUDA(cudaFuncSetAttribute(focal_finalize_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tile),
-                  "cudaFuncSetAttribute(focal finalize)");
-  focal_finalize_kernel<<<dim3(X, P), 256, tile, s>>>(focal, ix, wx, KX, iy, wy, KY, axial, scale, Z, H, W, X, Y, psf,
-                                                      energies);
-  MM_CHECK_LAUNCH("focal finalize");
+  if (!identity) {
+    if (tile > 48 * 1024)
+      MM_CHECK_CUDA(cudaFuncSetAttribute(focal_finalize_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tile),
+                    "cudaFuncSetAttribute(focal finalize)");
+    focal_finalize_kernel<<<dim3(X, P), 256, tile, s>>>(focal, ix, wx, KX, iy, wy, KY, axial, scale, Z, H, W, X, Y,
+                                                        psf, energies);
+    MM_CHECK_LAUNCH("focal finalize");
+  }
   if (psf_sum && psf_abs_sum && psf) {
     const long long E = (long long)X * Y * Z;
     MM_CHECK_CUDA(cudaMemsetAsync(psf_sum, 0, sizeof(double) * E, s), "zero psf sum");

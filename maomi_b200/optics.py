@@ -92,7 +92,6 @@ def pupil(config, *, custom_phase=None, phase_units="radians", phase_aperture="o
         raise ValueError("Explicit phase_units / phase_aperture required")
     n, d1, rad, objrad, k, fl = _pupil_grid(config)
     desc = _lib.PupilDesc(n=n, pitch=d1, beam_radius=rad, aperture=objrad, k=k, focal_length=fl)
-    keep = []
     if custom_phase is None and len(config.zernike_weights):
         abb = np.asarray(config.zernike_weights, dtype=float).ravel() * config.wavelength_um * 1e-6
         modes = [int(i) for i in np.nonzero(abb)[0]]
@@ -110,14 +109,12 @@ def pupil(config, *, custom_phase=None, phase_units="radians", phase_aperture="o
         arrays = [_lib.host_array(coef, _lib.c_double), _lib.host_array(mm, _lib.c_int),
                   _lib.host_array(mcos, _lib.c_int), _lib.host_array(ntm, _lib.c_int),
                   _lib.host_array(tcoef, _lib.c_double), _lib.host_array(tpow, _lib.c_int)]
-        keep += arrays
         desc.nmodes = len(modes)
         (desc.mode_coef, desc.mode_m, desc.mode_cos, desc.mode_nterms, desc.term_coef, desc.term_pow) = arrays
     if custom_phase is not None:
-        ph = torch.as_tensor(np.ascontiguousarray(custom_phase, np.float32), device=device)
+        ph = _lib.upload(np.ascontiguousarray(custom_phase, np.float32), device)
         if ph.ndim != 2:
             raise ValueError("custom_phase must be a 2-D array")
-        keep.append(ph)
         na = config.objNA if phase_aperture == "objective" else config.NA
         desc.custom_phase = ph.data_ptr()
         desc.custom_h, desc.custom_w = ph.shape
@@ -125,8 +122,9 @@ def pupil(config, *, custom_phase=None, phase_units="radians", phase_aperture="o
         desc.custom_scale = 2 * np.pi if phase_units == "waves" else 1.0
     out = torch.empty((n, n), dtype=torch.complex64, device=device)
     scratch = torch.empty(n * n + 2 * 1024 + 8, dtype=torch.float64, device=device)
+    # mm_pupil copies the host tables into the launch parameters before it
+    # returns, and the device buffers are stream-ordered: no synchronisation
     _lib.check(_lib.load().mm_pupil(desc, _lib.ptr(out), _lib.ptr(scratch), _lib.stream_of(device)), "pupil")
-    torch.cuda.current_stream(device).synchronize()  # host arrays in `keep` must outlive the launch
     return out
 
 

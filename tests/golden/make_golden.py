@@ -335,9 +335,58 @@ def make_rana_files(torch):
     return {"field_kernels": k, "bank_kernels": ks, "x_um": x, "y_um": y}
 
 
+def make_scanning(torch):
+    """The reference's static and per-frame scan operators on seeded inputs:
+    ``zstack`` (maomi/scanning.py:8-53, both modes, with and without masks, FP64
+    and FP32), ``single_scan`` with ``psf_fft`` (maomi/movie.py:37-66, grouped
+    and ungrouped) and ``blurred_background`` (movie.py:69-102, spatial and
+    frequency kernels)."""
+    from maomi.movie import blurred_background, psf_fft, single_scan
+    from maomi.scanning import zstack
+    rng = np.random.default_rng(909)
+    out = {}
+    # odd/even kernel sizes, kernels wider than half the volume, ragged Z
+    cases = [((23, 30, 17), (6, 5, 7)), ((32, 32, 12), (9, 10, 4)), ((40, 36, 9), (33, 33, 9))]
+    for i, (vs, ks) in enumerate(cases):
+        v = rng.uniform(0, 1, vs)
+        p = rng.uniform(0, 1, ks)
+        m1 = rng.uniform(0.5, 1.5, vs[:2])
+        m2 = rng.uniform(0.2, 1.0, vs[:2])
+        out[f"z{i}_volume"], out[f"z{i}_psf"], out[f"z{i}_mask"], out[f"z{i}_colmask"] = v, p, m1, m2
+        out[f"z{i}_convn64"] = zstack(v, p, mask=m1, collection_mask=m2).numpy()
+        out[f"z{i}_convn32"] = zstack(v.astype(np.float32), p.astype(np.float32), mask=m1,
+                                      collection_mask=m2).numpy()
+        out[f"z{i}_plain64"] = zstack(v, p).numpy()
+        out[f"z{i}_legacy64"] = zstack(v, p, mode="legacy_circular").numpy()
+    # single_scan: slab depth == PSF depth, grouped planes
+    for i, (vs, ks) in enumerate([((30, 26, 8), (7, 6, 8)), ((48, 40, 9), (12, 11, 9))]):
+        v = rng.uniform(0, 1, vs).astype(np.float32)
+        p = rng.uniform(0, 1, ks).astype(np.float32)
+        out[f"s{i}_volume"], out[f"s{i}_psf"] = v, p
+        for g in (1, 2, 3):
+            out[f"s{i}_g{g}"] = single_scan(v, p, scan_avg=g)
+            out[f"s{i}_g{g}_freq"] = single_scan(v, p, scan_avg=g, frequency_psf=psf_fft(v.shape, p, g))
+    # blurred_background: frame volume, planes above / below a slab, tail kernel
+    v = rng.uniform(0, 1, (36, 28, 14)).astype(np.float32)
+    extra = rng.uniform(0, 1, v.shape).astype(np.float32)
+    kern = rng.uniform(0, 1, (16, 16)).astype(np.float32)
+    kern /= kern.sum()
+    mask = rng.uniform(0.5, 1.5, v.shape[:2]).astype(np.float32)
+    zs = rng.uniform(0.5, 2.0, 9)
+    out.update(b_volume=v, b_extra=extra, b_kernel=kern, b_mask=mask, b_zscale=zs)
+    for name, idx in (("top", np.arange(5)), ("bottom", np.arange(9, 14))):
+        kw = dict(power_ratio=0.37, mask=mask, zscale=zs[:len(idx)], extra_volumes=[extra])
+        out[f"b_{name}_spatial"] = blurred_background(v, idx, kern, **kw)
+        spec = psf_fft(v.shape, kern)
+        out[f"b_{name}_freq"] = blurred_background(v, idx, spec, frequency=True, **kw)
+        out[f"b_{name}_freq_shape"] = np.asarray(spec.shape)
+    return out
+
+
 MAKERS = (("numerics", make_numerics), ("local_fft", make_local_fft), ("stage_small", make_stage_small),
           ("stage_reftest", make_stage_reftest), ("stage_bench_sites", make_stage_bench_sites),
-          ("fields", make_fields), ("stage_bench_lattice", make_stage_bench_lattice), ("rana_files", make_rana_files))
+          ("fields", make_fields), ("stage_bench_lattice", make_stage_bench_lattice), ("rana_files", make_rana_files),
+          ("scanning", make_scanning))
 
 
 def main(ref_path, only=None):

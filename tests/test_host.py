@@ -149,7 +149,8 @@ def test_descriptor_layouts_match_the_library():
     for name, cls in (("mm_stage_desc", _lib.StageDesc), ("mm_stage_plan", _lib.StagePlan),
                       ("mm_item_class", _lib.ItemClass), ("mm_pupil_desc", _lib.PupilDesc),
                       ("mm_base_desc", _lib.BaseDesc), ("mm_local_desc", _lib.LocalDesc),
-                      ("mm_surrogate_desc", _lib.SurrogateDesc)):
+                      ("mm_surrogate_desc", _lib.SurrogateDesc), ("mm_scan_planes", _lib.ScanPlanes),
+                      ("mm_scan_desc", _lib.ScanDesc), ("mm_scan_conv", _lib.ScanConv)):
         assert lib.mm_struct_size(name.encode()) == ctypes.sizeof(cls), name
     assert lib.mm_struct_size(b"nothing") == 0
 
