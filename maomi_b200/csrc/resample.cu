@@ -103,25 +103,41 @@ __global__ void focal_transpose_kernel(const float* __restrict__ focal, const fl
   const int rows = min(kFocalRows, X - x0);
   const int ry = rows * Y;
   const float* src = focal + (size_t)p * Z * X * Y + (size_t)x0 * Y;
+  const int tid = threadIdx.x, nt = blockDim.x;
   double acc = 0.0;
-  for (int e = threadIdx.x; e < Z * ry; e += blockDim.x) {
-    const int z = e / ry, o = e - z * ry;  // o = r * Y + y
-    const float v = scale * __ldg(src + (size_t)z * X * Y + o) * __ldg(axial + z);
-    tile[o * (Z + 1) + z] = v;
-    acc += v;
+  // planes outer, kFocalBatch of them in flight per thread: every load of a
+  // batch is issued before any is used, and no index needs a division
+  constexpr int kFocalBatch = 16;
+  for (int o = tid; o < ry; o += nt) {
+    for (int z0 = 0; z0 < Z; z0 += kFocalBatch) {
+      float v[kFocalBatch];
+#pragma unroll
+      for (int u = 0; u < kFocalBatch; ++u)
+        v[u] = z0 + u < Z ? __ldg(src + (size_t)(z0 + u) * X * Y + o) : 0.f;
+#pragma unroll
+      for (int u = 0; u < kFocalBatch; ++u) {
+        if (z0 + u >= Z) break;
+        const float w = scale * v[u] * __ldg(axial + z0 + u);
+        tile[o * (Z + 1) + z0 + u] = w;
+        acc += w;
+      }
+    }
   }
   __syncthreads();
   if (psf) {
+    // one warp per output run of Z values (z fastest): contiguous stores
     float* dst = psf + ((size_t)p * X + x0) * Y * Z;
-    for (int e = threadIdx.x; e < ry * Z; e += blockDim.x) dst[e] = tile[(e / Z) * (Z + 1) + e % Z];
+    const int lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
+    for (int o = warp; o < ry; o += nw)
+      for (int z = lane; z < Z; z += 32) dst[(size_t)o * Z + z] = tile[o * (Z + 1) + z];
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  if ((tid & 31) == 0) red[tid >> 5] = acc;
   __syncthreads();
-  if (threadIdx.x == 0) {
+  if (tid == 0) {
     double s = 0.0;
-    for (int w = 0; w < int(blockDim.x >> 5); ++w) s += red[w];
+    for (int w = 0; w < int(nt >> 5); ++w) s += red[w];
     atomicAdd(energies + p, s);
   }
 }
@@ -234,8 +250,9 @@ extern "C" int mm_focal_finalize(const float* focal, const int32_t* ix, const fl
     if (tt > 48 * 1024)
       MM_CHECK_CUDA(cudaFuncSetAttribute(focal_transpose_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tt),
                     "cudaFuncSetAttribute(focal transpose)");
-    focal_transpose_kernel<<<dim3((X + kFocalRows - 1) / kFocalRows, P), 256, tt, s>>>(focal, axial, scale, Z, X, Y,
-                                                                                          psf, energies);
+    const int threads = std::min(512, (std::min(kFocalRows, X) * Y + 31) / 32 * 32);  // one output run each
+    focal_transpose_kernel<<<dim3((X + kFocalRows - 1) / kFocalRows, P), threads, tt, s>>>(focal, axial, scale, Z, X,
+                                                                                              Y, psf, energies);
     MM_CHECK_LAUNCH("focal transpose");
   }
   const size_t tile = sizeof(float) * (size_t)Y * (Z + 1);

@@ -215,14 +215,18 @@ __global__ void __launch_bounds__(256) green_eval_table_kernel(const double* __r
 // solves the diagonal block, then every thread updates its rows with the
 // block's 32 columns (consecutive threads read consecutive rows: coalesced).
 constexpr int kSolveBlock = 32;
+// One CTA per (system b, right-hand side blockIdx.y): the columns are
+// independent, so each runs its own substitution chain (the same operations
+// in the same order as a CTA that carries all columns together).
 __global__ void __launch_bounds__(512) lu_solve_kernel(const double* __restrict__ lu, const int* __restrict__ piv,
-                                                        int m, int C, double* __restrict__ x) {
-  extern __shared__ double xs[];  // m x C, then m pivots
+                                                        int m, int ldx, double* __restrict__ x) {
+  constexpr int C = 1;
+  extern __shared__ double xs[];  // m values of this column, then m pivots
   int* sp = reinterpret_cast<int*>(xs + (size_t)m * C);
-  const int b = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int b = blockIdx.x, col = blockIdx.y, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const double* A = lu + (size_t)b * m * m;
-  double* xb = x + (size_t)b * m * C;
-  for (int e = tid; e < m * C; e += blockDim.x) xs[e] = xb[e];
+  double* xb = x + (size_t)b * m * ldx + col;
+  for (int e = tid; e < m; e += blockDim.x) xs[e] = xb[(size_t)e * ldx];
   for (int e = tid; e < m; e += blockDim.x) sp[e] = piv[(size_t)b * m + e];
   __syncthreads();
   if (tid == 0) {
@@ -243,15 +247,15 @@ __global__ void __launch_bounds__(512) lu_solve_kernel(const double* __restrict_
     if (warp == 0) {
       // the block's 32 x 32 L tile in registers (lane = row), x rows in registers
       const int i = kb + lane;
-      double lr[kSolveBlock], xr[4];
+      double lr[kSolveBlock], xr[C];
 #pragma unroll
       for (int kk = 0; kk < kSolveBlock; ++kk) lr[kk] = (i < ke && kb + kk < ke) ? A[(size_t)(kb + kk) * m + i] : 0.0;
 #pragma unroll
-      for (int c = 0; c < 4; ++c) xr[c] = (c < C && i < ke) ? xs[i * C + c] : 0.0;
+      for (int c = 0; c < C; ++c) xr[c] = (c < C && i < ke) ? xs[i * C + c] : 0.0;
 #pragma unroll
       for (int kk = 0; kk < kSolveBlock; ++kk) {
 #pragma unroll
-        for (int c = 0; c < 4; ++c) {
+        for (int c = 0; c < C; ++c) {
           const double xk = __shfl_sync(0xffffffffu, xr[c], kk);
           if (lane > kk) xr[c] -= lr[kk] * xk;
         }
@@ -278,16 +282,16 @@ __global__ void __launch_bounds__(512) lu_solve_kernel(const double* __restrict_
     const int kb = max(ke - kSolveBlock, 0);
     if (warp == 0) {
       const int i = kb + lane;
-      double ur[kSolveBlock], xr[4];
+      double ur[kSolveBlock], xr[C];
 #pragma unroll
       for (int kk = 0; kk < kSolveBlock; ++kk) ur[kk] = (i < ke && kb + kk < ke) ? A[(size_t)(kb + kk) * m + i] : 1.0;
 #pragma unroll
-      for (int c = 0; c < 4; ++c) xr[c] = (c < C && i < ke) ? xs[i * C + c] : 0.0;
+      for (int c = 0; c < C; ++c) xr[c] = (c < C && i < ke) ? xs[i * C + c] : 0.0;
 #pragma unroll
       for (int kk = kSolveBlock - 1; kk >= 0; --kk) {
         if (kb + kk >= ke) continue;
 #pragma unroll
-        for (int c = 0; c < 4; ++c) {
+        for (int c = 0; c < C; ++c) {
           if (lane == kk) xr[c] /= ur[kk];
           const double xk = __shfl_sync(0xffffffffu, xr[c], kk);
           if (lane < kk) xr[c] -= ur[kk] * xk;
@@ -310,7 +314,7 @@ __global__ void __launch_bounds__(512) lu_solve_kernel(const double* __restrict_
     }
     __syncthreads();
   }
-  for (int e = tid; e < m * C; e += blockDim.x) xb[e] = xs[e];
+  for (int e = tid; e < m; e += blockDim.x) xb[(size_t)e * ldx] = xs[e];
 }
 
 int eval_all(const double* p, const double* coef, int n, const double* q, int m, int Y, int ncoef, double* out,
@@ -416,12 +420,12 @@ extern "C" int mm_lu_solve_batched(const double* lu, const int* pivots, int batc
                                    void* stream) {
   MM_CHECK_ARG(lu && pivots && x, "NULL pointer");
   MM_CHECK_ARG(batch >= 1 && m >= 1 && nrhs >= 1 && nrhs <= 4, "bad LU solve sizes (1..4 right-hand sides)");
-  const size_t smem = sizeof(double) * (size_t)m * nrhs + sizeof(int) * (size_t)m;
-  MM_CHECK_ARG(smem <= 200 * 1024, "LU solve: %d x %d right-hand sides exceed shared memory", m, nrhs);
+  const size_t smem = sizeof(double) * (size_t)m + sizeof(int) * (size_t)m;
+  MM_CHECK_ARG(smem <= 200 * 1024, "LU solve: systems of %d unknowns exceed shared memory", m);
   if (smem > 48 * 1024)
     MM_CHECK_CUDA(cudaFuncSetAttribute(lu_solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
                   "cudaFuncSetAttribute(lu solve)");
-  lu_solve_kernel<<<batch, 512, smem, static_cast<cudaStream_t>(stream)>>>(lu, pivots, m, nrhs, x);
+  lu_solve_kernel<<<dim3(batch, nrhs), 512, smem, static_cast<cudaStream_t>(stream)>>>(lu, pivots, m, nrhs, x);
   MM_CHECK_LAUNCH("LU solve");
   return MM_OK;
 }

@@ -54,6 +54,8 @@ def field_shapes(config):
 
 
 _SIDE_STREAMS = {}
+#: per device, an event after the most recent persistent propagation launch
+_LAST_PROPAGATION = {}
 RESERVE_SMS = 0   # SMs the persistent kernel leaves to the overlapped v4 factorisation
 # Sites in flight in the persistent schedule: 96 (94 after balancing 4,225
 # sites into 45 waves) measured 3 % faster than 64 and than 128 on the
@@ -137,8 +139,11 @@ def stage_device(config, raw_fields, points_um=None, *, uin=None, device="cuda",
     tail ``profiles``/``weights``/``convmask``) plus the plan.  ``events``
     (a pair of CUDA events) brackets the propagation launch.  The v4 system
     depends on the site positions only; it is factored on a high-priority side
-    stream first, so it runs while the host prepares the plan (and on the
-    ``reserve_sms`` SMs the persistent kernel can leave to it)."""
+    stream that waits only for the previous stage's propagation launch, so it
+    runs beside that stage's reductions and this stage's preparation; the
+    propagation launch waits for it (unless ``reserve_sms`` SMs are left to
+    it), because factorisation kernels running beside the persistent launch
+    hold SMs it would otherwise use."""
     import torch
     from .backends.cuda.batched import OpticalPlan, trapezoid
     _lib.require_cuda(device)
@@ -150,16 +155,29 @@ def stage_device(config, raw_fields, points_um=None, *, uin=None, device="cuda",
         main = torch.cuda.current_stream(dev)
         factor = None
         if len(points) > 1:
+            # the factorisation depends on the host-side site positions only:
+            # it waits for the last persistent launch queued on this device
+            # (not for the reductions behind it), so it runs beside them
             side = _side_stream(dev)
-            side.wait_stream(main)
+            last = _LAST_PROPAGATION.get(str(torch.device(dev)))
+            if last is not None:
+                side.wait_event(last)
             with torch.cuda.stream(side):
                 factor = v4_factor_device(points * config.vres, device=dev)
         if plan is None:
             plan = OpticalPlan(config, raw_fields, uin=uin, device=device, precision=precision)
         pts, off = plan.offsets(points)
         P = len(pts)
+        if factor is not None and not reserve_sms:
+            # the factorisation's kernels take whole SMs from the persistent
+            # launch if they overlap it: let them finish first (they overlap
+            # the previous stage's reductions and this stage's preparation)
+            main.wait_stream(side)
         res = plan.run_sites(off, tail_per_site=False, slots=slots, schedule=schedule, check=check, events=events,
                              reserve_sms=reserve_sms if factor is not None else 0)
+        done = torch.cuda.Event()
+        done.record(main)
+        _LAST_PROPAGATION[str(torch.device(dev))] = done
         psf, energies, s1, s2 = plan.finalize_focal(res["focal"], psf=True, sums=True)
         prof, wts = [], []
         for j in range(2):
