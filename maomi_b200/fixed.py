@@ -372,55 +372,131 @@ def run_stage(config, raw_fields, points_um=None, *, uin=None, device="cuda", ta
     return stage_to_host(config, dev, return_psf_3d=return_psf_3d)
 
 
+
+
+def _multibeam(config, volume, input_pupil, beam_weights, opts):
+    """Incoherent channels (fixed.py:237-285): one stage per named pupil on
+    shared raw fields; detected intensities add with nonnegative weights."""
+    from .fields import prepare_fields
+    if opts["custom_phase"] is not None:
+        raise ValueError("Compose channel pupil phases explicitly")
+    if not input_pupil:
+        raise ValueError("At least one beam required")
+    weights = {k: 1.0 for k in input_pupil} if beam_weights is None else dict(beam_weights)
+    if (set(weights) != set(input_pupil) or not all(np.isfinite(w) and w >= 0 for w in weights.values())
+            or sum(weights.values()) <= 0):
+        raise ValueError("Nonnegative detected-intensity weight per beam required")
+    start = time.perf_counter()
+    _lib.require_cuda(opts["device"])
+    raw = (prepare_fields(config, opts["vessels"], scatter=opts["scatter"], device=opts["device"])
+           if opts["raw_fields"] is None else opts["raw_fields"])
+    keep = ("vessels", "tails", "batch_size", "count_per_axis", "mask_mode", "device", "render_image")
+    channels = {name: run_fixed(config, volume, raw_fields=raw, input_pupil=field, **{k: opts[k] for k in keep})
+                for name, field in input_pupil.items()}
+    points = fixed_locations(config, opts["count_per_axis"])
+    out = {"channels": channels, "beam_weights": weights, "points_um": points,
+           "unique_optical_paths": len(points) * len(channels), "unique_optical_positions": len(points),
+           "total_seconds": time.perf_counter() - start,
+           "settings": {"combination": "incoherent detected-intensity sum", "scaling": config.scaling,
+                        "paths_per_position": len(channels), "count_per_axis": opts["count_per_axis"],
+                        "mask_mode": opts["mask_mode"]}}
+    if opts["render_image"]:
+        out["image"] = sum(weights[k] * v["image"] for k, v in channels.items())
+    return out
+
+
 def run_fixed(config, volume=None, *, vessels=None, raw_fields=None, scatter=True, custom_phase=None,
               phase_units="radians", phase_aperture="objective", input_pupil=None, beam_weights=None, tails=True,
               batch_size=32, count_per_axis=65, mask_mode="matlab_v4", device="cuda", rana=False,
-              render_image=False):
-    """Optical stage on the fixed lattice (maomi/fixed.py:193-411 without the
-    input-generation and static-scan stages, which lie outside this package).
+              render_image=True):
+    """MATLAB v4 masks and arithmetic PSF averaging on the fixed site lattice
+    (maomi/fixed.py:193-411), every stage on the GPU.
 
-    ``raw_fields`` must be supplied; ``render_image`` and ``rana`` belong to the
-    downstream renderer and are not provided here."""
-    from .optics import pupil
+    Raw fields are generated on the device when not supplied
+    (``maomi_b200.fields.prepare_fields``; its noise is a device draw from
+    ``config.seed``, not the reference's CPU stream), the collection mask is
+    built from ``vessels``, a mapping of pupils runs incoherent channels, and
+    ``render_image`` convolves the masked volume with the mean PSF
+    (``maomi_b200.scanning.zstack``).  ``batch_size`` is the number of sites in
+    flight.  The RANA attach branch belongs to the reference's RANA add-on
+    package and is not provided (``rana`` must be False or None)."""
+    from .fields import prepare_fields
+    from .optics import collection_mask, pupil
+    from .scanning import zstack
+    if rana is not False and rana is not None:
+        raise ValueError("the RANA add-on attach path is not part of maomi_b200.run_fixed; render with "
+                         "maomi_b200.rana.RanaOperator over the returned psf_3d")
     if mask_mode != "matlab_v4":
-        raise ValueError("run_fixed requires matlab_v4")
-    if raw_fields is None:
-        raise ValueError("raw_fields are required (scattering-field generation is not part of this package)")
-    if render_image or (rana is not False and rana is not None):
-        raise ValueError("static scanning and RANA rendering are not part of run_fixed here; "
-                         "use maomi_b200.rana for the local-PSF renderer")
+        raise ValueError("run_fixed requires matlab_v4; use maomi.enhanced.CubicFullFieldRenderer "
+                         "with a complete custom FullFieldPSF for cubic imaging")
+    if isinstance(input_pupil, dict):
+        return _multibeam(config, volume, input_pupil, beam_weights,
+                          dict(vessels=vessels, raw_fields=raw_fields, scatter=scatter, custom_phase=custom_phase,
+                               tails=tails, batch_size=batch_size, count_per_axis=count_per_axis,
+                               mask_mode=mask_mode, device=device, render_image=render_image))
     if beam_weights is not None:
         raise ValueError("beam_weights requires a mapping of pupils")
-    if not isinstance(batch_size, int) or batch_size < 1:
-        raise ValueError("batch_size must be a positive integer")
-    if input_pupil is not None and custom_phase is not None:
-        raise ValueError("Supply either input_pupil or custom_phase; compose the field explicitly")
-    expected = field_shapes(config)
-    if len(raw_fields) != 3 or any(tuple(np.shape(a)) != tuple(s) for a, s in zip(raw_fields, expected)):
-        raise ValueError(f"Raw A/B/C fields must have shapes {expected}")
-    if any(np.iscomplexobj(a) or not np.isfinite(np.asarray(a)).all() for a in raw_fields):
-        raise ValueError("Raw refractive-index fields must be finite and real")
+    if not str(device).startswith("cuda"):
+        raise ValueError("Fixed fast pipeline requires CUDA; use maomi.optics for CPU reference calculations")
     _lib.require_cuda(device)
     import torch
+    if isinstance(batch_size, bool) or not isinstance(batch_size, int) or batch_size < 1:
+        raise ValueError("batch_size must be a positive integer")
+    if phase_units not in ("radians", "waves") or phase_aperture not in ("objective", "excitation"):
+        raise ValueError("Invalid pupil phase units/aperture")
+    if input_pupil is not None and custom_phase is not None:
+        raise ValueError("Supply either input_pupil or custom_phase; compose the field explicitly")
+    expected = tuple(int(v) for v in np.round(np.asarray(config.volume_um) * config.vres).astype(int))
+    if render_image:
+        vol = volume if isinstance(volume, torch.Tensor) else np.asarray(volume, np.float32)
+        if tuple(vol.shape) != expected or not bool(np.isfinite(np.asarray(vol.cpu() if isinstance(
+                vol, torch.Tensor) else vol)).all()):
+            raise ValueError(f"Expected finite volume of shape {expected}")
     started = time.perf_counter()
     timings = {}
+    supplied = raw_fields is not None
+    t = time.perf_counter()
+    raw = prepare_fields(config, vessels, scatter=scatter, device=device) if raw_fields is None else raw_fields
+    shapes = field_shapes(config)
+    if len(raw) != 3 or any(tuple(np.shape(a)) != tuple(s) for a, s in zip(raw, shapes)):
+        raise ValueError(f"Raw A/B/C fields must have shapes {shapes}")
+    for a in raw:
+        if (a.is_complex() if isinstance(a, torch.Tensor) else np.iscomplexobj(a)) or not bool(
+                (torch.isfinite(a).all() if isinstance(a, torch.Tensor) else np.isfinite(np.asarray(a)).all())):
+            raise ValueError("Raw refractive-index fields must be finite and real")
+    col = (collection_mask(vessels, config, device=device) if vessels is not None
+           else np.ones(expected[:2], np.float32))
+    timings["fields_and_collection"] = time.perf_counter() - t
     t = time.perf_counter()
     u = (pupil(config, custom_phase=custom_phase, phase_units=phase_units, phase_aperture=phase_aperture,
                device=device) if input_pupil is None
-         else torch.as_tensor(input_pupil, dtype=torch.complex64, device=device))
+         else torch.as_tensor(input_pupil, dtype=torch.complex64).to(device))
+    v, _ = config.parameters()
+    n = int(round((v.vasc_sz[0] - config.volume_um[0]) * config.vres * config.ss))
+    if tuple(u.shape) != (n, n) or not bool(torch.isfinite(u).all()) or not bool((u.abs() > 0).any()):
+        raise ValueError("Input pupil must be a finite nonzero complex field on the optical grid")
     from .backends.cuda.batched import OpticalPlan
-    plan = OpticalPlan(config, raw_fields, uin=u, device=device)
+    plan = OpticalPlan(config, raw, uin=u, device=device)
     torch.cuda.synchronize(device)
     timings["plan"] = time.perf_counter() - t
     t = time.perf_counter()
-    result = run_stage(config, raw_fields, fixed_locations(config, count_per_axis), device=device, tails=tails,
-                       slots=max(batch_size, 1), plan=plan)
+    result = run_stage(config, raw, fixed_locations(config, count_per_axis), device=device, tails=tails,
+                       slots=batch_size, plan=plan)
+    result["colmask"] = col
     timings["propagation_and_aggregation"] = time.perf_counter() - t
+    t = time.perf_counter()
+    if render_image:
+        result["image"] = zstack(volume, result["psf"].astype(np.float32), mask=result["mask"].astype(np.float32),
+                                 collection_mask=col, device=device).cpu().numpy()
+    timings["static_scan"] = time.perf_counter() - t
     result["timing_seconds"] = timings
     result["total_seconds"] = time.perf_counter() - started
-    result["settings"] = {"seed": config.seed, "scaling": config.scaling, "fields": "provided",
-                          "phase_units": phase_units, "phase_aperture": phase_aperture,
+    result["settings"] = {"seed": config.seed, "scaling": config.scaling,
+                          "fields": "provided" if supplied else "generated",
+                          "scatter": None if supplied else bool(scatter), "phase_units": phase_units,
+                          "phase_aperture": phase_aperture,
                           "input_pupil": "provided" if input_pupil is not None else "gaussian",
-                          "count_per_axis": count_per_axis, "mask_mode": mask_mode,
-                          "psf_average": "arithmetic mean of absolute per-point PSFs"}
+                          "collection_absorption": vessels is not None, "tail_background_added_to_image": False,
+                          "count_per_axis": count_per_axis, "adaptive": False, "low_order_subtraction": False,
+                          "mask_mode": mask_mode, "psf_average": "arithmetic mean of absolute per-point PSFs"}
     return result

@@ -144,3 +144,76 @@ def propagate(config, raw_fields, points_um, *, uin=None, device="cuda", save_fu
     res["scattering_replay"] = "provided_raw_fields"
     res["phase_mode"] = "full"
     return res
+
+
+def _collection_disks(config, vessel_shape):
+    """(start, disk) per slab of ``pc`` vessel planes: the normalised disk of
+    the collection cone at the slab's mid depth (optics.py:390-404), or None
+    where the reference skips the slab (cone apex above it, or no pixel)."""
+    r = config.vres
+    pc = int(round(config.prop_um * r))
+    slope = np.tan(np.arcsin(config.objNA / config.n))
+    x = np.arange(-vessel_shape[0] / 2, vessel_shape[0] / 2)[:, None]
+    y = np.arange(-vessel_shape[1] / 2, vessel_shape[1] / 2)[None, :]
+    out = []
+    for start in range(0, vessel_shape[-1], pc):
+        radius = r * slope * (config.depth_um + config.volume_um[2] / 2 - (start / pc + 0.5) * config.prop_um)
+        inside = (x * x + y * y <= radius * radius) if radius > 0 else np.zeros((1, 1), bool)
+        rows, cols = np.nonzero(inside.any(1))[0], np.nonzero(inside.any(0))[0]
+        if not len(rows):
+            out.append((start, None))
+            continue
+        disk = inside[rows[0]:rows[-1] + 1, cols[0]:cols[-1] + 1].astype(np.float32)
+        out.append((start, disk / disk.sum()))
+    return out
+
+
+def collection_mask(vessels, config, *, device=None):
+    """NAOMi's depth-dependent collection disk and hemoglobin absorption
+    (maomi/optics.py:384-409) on the GPU.
+
+    Every slab of ``pc`` vessel planes is summed and convolved ('same',
+    centred as SciPy does) with the normalised disk of the collection cone at
+    the slab's depth; the slabs' disks share one kernel stack (each placed so
+    that one crop serves all), so the sum over slabs is one pass of the
+    plane-convolution engine; the centre crop of the FOV becomes the
+    transmission 10^(-total / vres * hemoabs).  Float32 like the reference;
+    NumPy vessels give a NumPy mask, device tensors a device tensor."""
+    import torch
+    from ._scan import KernelSpectrum, as_device, transform_size
+    dev = device if device is not None else (vessels.device if isinstance(vessels, torch.Tensor) and vessels.is_cuda
+                                             else "cuda")
+    _lib.require_cuda(dev)
+    v = as_device(vessels, dev, torch.float32)
+    if v.ndim != 3:
+        raise ValueError("vessels must be an X,Y,Z volume")
+    r = config.vres
+    pc = int(round(config.prop_um * r))
+    shape = np.round(np.array(config.volume_um[:2]) * r).astype(int)
+    off = (np.array(v.shape[:2]) - shape) // 2
+    disks = _collection_disks(config, tuple(v.shape))
+    live = [d for _, d in disks if d is not None]
+    if not live:
+        ones = torch.ones(tuple(int(s) for s in shape), dtype=torch.float32, device=dev)
+        return ones if isinstance(vessels, torch.Tensor) else ones.cpu().numpy()
+    # one crop for every slab: disk (dx, dy) with SciPy's 'same' start
+    # (d - 1)//2 sits at offset C - (d - 1)//2 of a common frame
+    cx = max((d.shape[0] - 1) // 2 for d in live)
+    cy = max((d.shape[1] - 1) // 2 for d in live)
+    kx = max(cx - (d.shape[0] - 1) // 2 + d.shape[0] for d in live)
+    ky = max(cy - (d.shape[1] - 1) // 2 + d.shape[1] for d in live)
+    stack = np.zeros((kx, ky, len(disks)), np.float32)
+    for s, (_, d) in enumerate(disks):
+        if d is not None:
+            ox, oy = cx - (d.shape[0] - 1) // 2, cy - (d.shape[1] - 1) // 2
+            stack[ox:ox + d.shape[0], oy:oy + d.shape[1], s] = d
+    crop = (cx + int(off[0]), cy + int(off[1]))
+    X, Y = int(shape[0]), int(shape[1])
+    # every source row must fit the transform as well as the kept window
+    fx = transform_size(max(crop[0] + X, v.shape[0] + kx - 1 - crop[0], v.shape[0]))
+    fy = transform_size(max(crop[1] + Y, v.shape[1] + ky - 1 - crop[1], v.shape[1]))
+    spec = KernelSpectrum(_lib.upload(stack, dev), fx, fy)
+    total = torch.empty((X, Y), dtype=torch.float32, device=dev)
+    spec.convolve(v, zrule=_lib.MM_SCAN_SUM_Z, out=total, crop=crop, out_shape=(X, Y), out_planes=1, group=pc)
+    mask = torch.pow(10.0, -total / r * config.hemoabs)
+    return mask if isinstance(vessels, torch.Tensor) else mask.cpu().numpy()

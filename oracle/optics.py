@@ -559,3 +559,47 @@ def locations(volume_um, count_per_axis):
     x = np.linspace(0, volume_um[0], count_per_axis) if count_per_axis > 1 else np.array([volume_um[0] / 2])
     y = np.linspace(0, volume_um[1], count_per_axis) if count_per_axis > 1 else np.array([volume_um[1] / 2])
     return np.stack(np.meshgrid(x, y, indexing="ij"), -1).reshape(-1, 2)
+
+
+def collection_disks(cfg, vessel_shape):
+    """Normalised collection disks per slab of ``pc`` vessel planes, or None
+    for slabs the reference skips (optics.py:384-404): (start, disk) pairs."""
+    r = cfg.vres
+    pc = int(round(cfg.prop_um * r))
+    out = []
+    for start in range(0, vessel_shape[-1], pc):
+        depth = (start / pc + 0.5) * cfg.prop_um
+        radius = r * np.tan(np.arcsin(cfg.objNA / cfg.n)) * (cfg.depth_um + cfg.volume_um[2] / 2 - depth)
+        if radius <= 0:
+            out.append((start, None))
+            continue
+        x = np.arange(-vessel_shape[0] / 2, vessel_shape[0] / 2)[:, None]
+        y = np.arange(-vessel_shape[1] / 2, vessel_shape[1] / 2)[None, :]
+        disk = (x * x + y * y <= radius * radius).astype(np.float64)
+        nz = np.argwhere(disk)
+        if len(nz) == 0:
+            out.append((start, None))
+            continue
+        lo, hi = nz.min(0), nz.max(0) + 1
+        disk = disk[lo[0]:hi[0], lo[1]:hi[1]]
+        out.append((start, disk / disk.sum()))
+    return out
+
+
+def collection_mask(vessels, cfg):
+    """optics.py:384-409 in float64: per slab, the vessel occupancy summed over
+    the slab convolved ('same', SciPy's centring) with the normalised disk of
+    the collection cone at the slab's depth; the centre FOV crop of the sum,
+    as hemoglobin transmission 10^(-total / vres * hemoabs)."""
+    from scipy.signal import fftconvolve
+    a = np.asarray(vessels, np.float64)
+    r = cfg.vres
+    pc = int(round(cfg.prop_um * r))
+    total = np.zeros(a.shape[:2])
+    for start, disk in collection_disks(cfg, a.shape):
+        if disk is not None:
+            total += fftconvolve(a[..., start:start + pc].sum(-1), disk, mode="same")
+    shape = np.round(np.array(cfg.volume_um[:2]) * r).astype(int)
+    off = (np.array(total.shape) - shape) // 2
+    total = total[off[0]:off[0] + shape[0], off[1]:off[1] + shape[1]]
+    return 10 ** (-total / r * cfg.hemoabs)

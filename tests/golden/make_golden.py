@@ -383,10 +383,38 @@ def make_scanning(torch):
     return out
 
 
+def make_collection(torch):
+    """The reference's collection mask (maomi/optics.py:384-409) and its
+    vessel-aware scattering fields (optics.py:120-197, zero scatter) for seeded
+    vessel occupancies on two geometries: the reference's own test geometry
+    and the small benchmark-recipe geometry."""
+    from maomi.optics import OpticalConfig, collection_mask, prepare_fields
+    sys.path.insert(0, str(REPO))
+    from maomi_b200 import synthetic
+    out = {}
+    cfgs = [OpticalConfig(volume_um=(16.0, 16.0, 10.0), depth_um=20.0, tail_um=10.0),
+            synthetic.small_stage_config(OpticalConfig)]
+    rng = np.random.default_rng(1234)
+    for i, cfg in enumerate(cfgs):
+        r = cfg.vres
+        shapes = [tuple(a.shape) for a in prepare_fields(cfg, scatter=False)]
+        za = int(round((cfg.depth_um + cfg.volume_um[2] / 2 - cfg.psf_um[2] / 2) * r))
+        zb = int(round(cfg.psf_um[2] * r))
+        nc = int(round(cfg.tail_um * r))
+        vshape = (shapes[0][0], shapes[0][1], za + zb + nc + 3)
+        ves = (rng.uniform(0, 1, vshape) > 0.85).astype(np.uint8)
+        out[f"c{i}_vessels"] = ves
+        out[f"c{i}_colmask"] = collection_mask(ves.astype(np.float32), cfg)
+        for j, a in enumerate(prepare_fields(cfg, ves.astype(np.float32), scatter=False)):
+            out[f"c{i}_raw{j}"] = a.numpy()
+        out.update({f"c{i}_cfg_" + k: v for k, v in _cfg_dict(cfg).items()})
+    return out
+
+
 MAKERS = (("numerics", make_numerics), ("local_fft", make_local_fft), ("stage_small", make_stage_small),
           ("stage_reftest", make_stage_reftest), ("stage_bench_sites", make_stage_bench_sites),
           ("fields", make_fields), ("stage_bench_lattice", make_stage_bench_lattice), ("rana_files", make_rana_files),
-          ("scanning", make_scanning))
+          ("scanning", make_scanning), ("collection", make_collection))
 
 
 def main(ref_path, only=None):

@@ -176,10 +176,14 @@ def test_product_refuses_cpu():
     raw = [np.zeros(s, np.float32) for s in field_shapes(cfg)]
     with pytest.raises(ValueError):
         OpticalPlan(cfg, raw, device="cpu")
-    with pytest.raises(ValueError):
-        run_fixed(cfg, raw_fields=[np.zeros((3, 3, 3), np.float32)] * 3)
-    with pytest.raises(ValueError):
-        run_fixed(cfg, raw_fields=None)
+    with pytest.raises(ValueError, match="requires CUDA"):
+        run_fixed(cfg, raw_fields=raw, device="cpu")
+    with pytest.raises(ValueError, match="requires CUDA"):
+        run_fixed(cfg, device="cpu", render_image=False)
+    with pytest.raises(ValueError, match="beam"):
+        run_fixed(cfg, input_pupil={}, device="cpu")
+    with pytest.raises(ValueError, match="mapping"):
+        run_fixed(cfg, beam_weights={"a": 1.0}, device="cpu")
 
 
 def test_lattice_index_detects_symmetric_lattices():
