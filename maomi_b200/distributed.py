@@ -65,15 +65,18 @@ def assemble_sharded(config, parts, count, group=None, *, points_um, z_positions
     tails = [sum_over_ranks(t.clone(), group) for t in parts["tail_sum"]]
     weights = [(p * torch.as_tensor(trapezoid(p.shape[1]), dtype=p.dtype, device=p.device)).sum(1) * config.prop_um
                for p in profiles]
-    values = torch.stack([energies, weights[0], weights[1]], 1).cpu().numpy()
+    values = torch.stack([energies, weights[0], weights[1]], 1)
     shape = tuple(int(v) for v in np.round(np.array(config.volume_um[:2]) * config.vres))
     pts = np.asarray(points_um, float)
     if solve is None:
-        from .numerics import v4_interpolate
-        q = np.stack(np.meshgrid(*[np.arange(k) + 0.5 for k in shape], indexing="ij"), -1)
-        masks = v4_interpolate(pts * config.vres, values, q)
+        # every rank factors, solves and evaluates the same v4 system on its
+        # own GPU (no further collective)
+        from .numerics import v4_evaluate_grid_device, v4_factor_device, v4_solve_device
+        dev = values.device
+        p_dev, coef = v4_solve_device(v4_factor_device(pts * config.vres, device=dev), values)
+        masks = v4_evaluate_grid_device(p_dev, coef, *shape, device=dev, points_host=pts * config.vres).cpu().numpy()
     else:
-        masks = solve(pts * config.vres, values, shape)
+        masks = solve(pts * config.vres, values.cpu().numpy(), shape)
     mask = masks[..., 0]
     mean = float(mask.mean())
     res = {"psf": (s2 / count).cpu().numpy(), "psf_raw": (s1 / count).cpu().numpy(), "points_um": pts,
@@ -90,22 +93,54 @@ def assemble_sharded(config, parts, count, group=None, *, points_um, z_positions
     return res
 
 
-def run_stage_sharded(config, raw_fields, points_um=None, *, group=None, device=None, precision="compensated", slots=96):
+def band_window(config, points_um, sizes):
+    """Raw-field rows a band of sites reads: per stage (window size in
+    ``sizes``) the rows [x0_min, x0_max + size) of the site windows, and the
+    band's points shifted so its first row is row 0.  Only for ss = 1 (the
+    phase preparation then reads each raw row alone; the bicubic resize of
+    ss > 1 mixes neighbouring rows at the crop edges)."""
+    pts = np.asarray(points_um, float).reshape(-1, 2)
+    x0 = np.round(pts[:, 0] * config.vres).astype(int)
+    lo = int(x0.min())
+    rows = [(lo, int(x0.max()) + int(s)) for s in sizes]
+    return rows, pts - np.array([lo / config.vres, 0.0])
+
+
+def band_stage(config, raw_fields, points_um, *, device, precision="compensated", slots=96, band_upload=True):
+    """Stage products of one band of sites, uploading only the raw rows the
+    band's windows touch (``band_window``); no v4 masks (see
+    ``assemble_sharded``).  Returns the ``fixed.stage_device`` dictionary."""
+    from ._propagation import geometry
+    from .fixed import stage_device
+    pts = np.asarray(points_um, float).reshape(-1, 2)
+    raw, local = raw_fields, pts
+    if band_upload and config.ss == 1:
+        g = geometry(config, raw_fields)
+        rows, local = band_window(config, pts, (g.n, g.n2, g.n))
+        raw = [a[r0:r1] for a, (r0, r1) in zip(raw_fields, rows)]
+    dev = stage_device(config, raw, local, device=device, slots=slots, precision=precision, masks=False)
+    dev["points_um"] = pts
+    return dev
+
+
+def run_stage_sharded(config, raw_fields, points_um=None, *, group=None, device=None, precision="compensated",
+                      slots=96, band_upload=True):
     """The optical stage of one tissue block on every rank of `group`, each
-    rank propagating its band of sites on its own GPU."""
+    rank propagating its contiguous band of sites on its own GPU from the raw
+    rows that band reads (plus the window halo), then the small exchange of
+    ``assemble_sharded`` and the v4 masks on every rank."""
     import torch
     import torch.distributed as dist
-    from .fixed import fixed_locations, stage_device
+    from .fixed import fixed_locations
     rank, world = dist.get_rank(group), dist.get_world_size(group)
     device = device or f"cuda:{torch.cuda.current_device()}"
     pts = fixed_locations(config) if points_um is None else np.asarray(points_um, float)
     lo, hi = shard(len(pts), rank, world)
-    dev = stage_device(config, raw_fields, pts[lo:hi], device=device, slots=slots, precision=precision)
+    dev = band_stage(config, raw_fields, pts[lo:hi], device=device, precision=precision, slots=slots,
+                     band_upload=band_upload)
     plan = dev["plan"]
-    tail_sum = []
-    for j in range(2):
-        conv = dev["convmask"][j] * (hi - lo)  # stage_device returns the band's mean image
-        tail_sum.append(conv)
+    # stage_device returns the band's mean tail image: scale back to its sum
+    tail_sum = [c * (hi - lo) for c in dev["convmask"]]
     parts = {"energies": dev["energies"], "profiles": dev["profiles"], "psf_sum": dev["psf_sum"],
              "psf_abs_sum": dev["psf_abs_sum"], "tail_sum": tail_sum}
     res = assemble_sharded(config, parts, len(pts), group, points_um=pts, z_positions=plan.z_positions, cut=plan.cut)

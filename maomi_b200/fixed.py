@@ -129,7 +129,7 @@ def assemble(config, out, shape, *, mask_mode="matlab_v4", z_positions=None, cut
 
 def stage_device(config, raw_fields, points_um=None, *, uin=None, device="cuda", tails=True, count_per_axis=65,
                  slots=SLOTS, schedule=None, plan=None, check=True, events=None, precision="compensated",
-                 reserve_sms=RESERVE_SMS):
+                 reserve_sms=RESERVE_SMS, masks=True):
     """Fused optical stage leaving every product on the device.
 
     Phase preparation (inside ``OpticalPlan``), the persistent propagation of
@@ -143,7 +143,9 @@ def stage_device(config, raw_fields, points_um=None, *, uin=None, device="cuda",
     runs beside that stage's reductions and this stage's preparation; the
     propagation launch waits for it (unless ``reserve_sms`` SMs are left to
     it), because factorisation kernels running beside the persistent launch
-    hold SMs it would otherwise use."""
+    hold SMs it would otherwise use.  ``masks=False`` skips the v4 masks
+    (``masks`` is then None): a sharded stage solves them once over every
+    rank's sites."""
     import torch
     from .backends.cuda.batched import OpticalPlan, trapezoid
     _lib.require_cuda(device)
@@ -154,7 +156,7 @@ def stage_device(config, raw_fields, points_um=None, *, uin=None, device="cuda",
     with torch.inference_mode():
         main = torch.cuda.current_stream(dev)
         factor = None
-        if len(points) > 1:
+        if masks and len(points) > 1:
             # the factorisation depends on the host-side site positions only:
             # it waits for the last persistent launch queued on this device
             # (not for the reductions behind it), so it runs beside them
@@ -186,7 +188,9 @@ def stage_device(config, raw_fields, points_um=None, *, uin=None, device="cuda",
             wts.append((pj * plan.tail_trapezoid[j]).sum(1) * config.prop_um)
         values = torch.stack([energies, wts[0], wts[1]] if tails else [energies], 1)
         shape = tuple(int(v) for v in np.round(np.array(config.volume_um[:2]) * config.vres))
-        if P > 1:
+        if not masks:
+            masks = None
+        elif P > 1:
             main.wait_stream(side)
             for t in factor.tensors():
                 t.record_stream(main)
