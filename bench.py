@@ -63,10 +63,12 @@ def parse():
                          "independent block per rank")
     ap.add_argument("--no-parity", action="store_true", help="skip the error report against the reference")
     ap.add_argument("--precision", default="compensated", choices=["compensated", "compensated-full", "mixed", "fp64", "fp32"])
-    ap.add_argument("--workload", default="stage", choices=["stage", "surrogate", "uneven", "local", "fields"],
+    ap.add_argument("--workload", default="stage", choices=["stage", "surrogate", "uneven", "local", "fields", "zstack",
+                                                                    "render"],
                     help="stage: the headline optical stage; surrogate: the learned PSF path with its plain gate; "
                          "uneven: 6,000 mixed-size items in one graph; local: the local-PSF render; "
-                         "fields: the raw A/B/C scattering fields of the benchmark geometry")
+                         "fields: the raw A/B/C scattering fields of the benchmark geometry; zstack: the static scan "
+                         "of the benchmark volume; render: the cubic-RBF depth renderer")
     ap.add_argument("--reserve-sms", type=int, default=None,
                     help="SMs the propagation leaves to the overlapped v4 factorisation (default: the library's)")
     ap.add_argument("--train-sites", type=int, default=20000)
@@ -481,6 +483,153 @@ def run_local(args):
           clocks=clk.summary(), **line_extra)
 
 
+def scan_bytes(X, Y, Z, kx, ky, kz, fx, fy, cbytes=8, rbytes=4):
+    """Bytes the plane-convolution engine moves for one zstack (matlab_convn)
+    call: every pass reads and writes its planes once (rows forward on the
+    X source rows, columns forward to all fx rows, the per-bin Z rule over
+    the source and kernel spectra, columns inverse keeping X rows, rows
+    inverse keeping Y columns), plus the kernel spectrum build."""
+    p_in, p_k = -(-Z // 2), -(-kz // 2)
+    half = fx * (fy // 2 + 1) * cbytes
+    kern = p_k * kx * fy * cbytes * 2 + p_k * fx * fy * cbytes * 2 + kz * half
+    vol = (X * Y * Z * rbytes + 2 * X * Y * rbytes + p_in * X * fy * cbytes          # rows forward
+           + p_in * X * fy * cbytes + p_in * fx * fy * cbytes                          # columns forward
+           + p_in * fx * fy * cbytes + kz * half + p_in * fx * fy * cbytes             # Z rule
+           + p_in * fx * fy * cbytes + p_in * X * fy * cbytes                          # columns inverse
+           + p_in * X * fy * cbytes + X * Y * Z * rbytes)                              # rows inverse
+    return kern + vol
+
+
+def run_zstack(args):
+    """The static scan of run_fixed at the benchmark size: zstack
+    (matlab_convn) of a 512 x 512 x 60 float32 volume with the 40 x 40 x 46
+    mean PSF, both XY masks, through the plane-convolution engine."""
+    import torch
+    from maomi_b200 import _lib
+    from maomi_b200._scan import transform_size
+    from maomi_b200.scanning import zstack
+    dev = "cuda:0"
+    torch.cuda.set_device(0)
+    stream = torch.cuda.current_stream(dev)
+    lib = _lib.load()
+    rng = np.random.default_rng(17)
+    X, Y, Z, kx, ky, kz = 512, 512, 60, 40, 40, 46
+    vol = rng.uniform(0, 1, (X, Y, Z)).astype(np.float32)
+    g = np.exp(-0.5 * (((np.arange(kx) - 20) / 4.0) ** 2)[:, None, None] - 0.5 * (((np.arange(ky) - 20) / 4.0) ** 2)[
+        None, :, None] - 0.5 * (((np.arange(kz) - 23) / 9.0) ** 2)[None, None, :])
+    psf = (g * rng.uniform(0.9, 1.1, g.shape)).astype(np.float32)
+    m1 = rng.uniform(0.5, 1.5, (X, Y)).astype(np.float32)
+    m2 = rng.uniform(0.8, 1.0, (X, Y)).astype(np.float32)
+    v_d, p_d, m1_d, m2_d = (torch.as_tensor(a, device=dev) for a in (vol, psf, m1, m2))
+    launches0 = lib.mm_launch_count()
+    with Clocks(0) as clk:
+        ms = _timed(lambda: zstack(v_d, p_d, mask=m1_d, collection_mask=m2_d, device=dev), args.steps, args.warmup,
+                    stream)
+    launches = (lib.mm_launch_count() - launches0) / (args.steps + args.warmup)
+
+    def e2e():
+        zstack(vol, psf, mask=m1, collection_mask=m2, device=dev).cpu()
+
+    e2e_ms = _timed(e2e, args.steps, 1, stream)
+    fx, fy = transform_size(X + kx // 2), transform_size(Y + ky // 2)
+    nbytes = scan_bytes(X, Y, Z, kx, ky, kz, fx, fy)
+    pk, pk_kind = peaks()
+    achieved = nbytes / (ms * 1e-3) / 1e9
+    extra = {}
+    got = zstack(v_d, p_d, mask=m1_d, collection_mask=m2_d, device=dev).cpu().numpy()
+    if not args.no_cpu_baseline:
+        from scipy import fft as sfft
+        from oracle import scanning as S
+        cores = os.cpu_count() or 1
+        t0 = time.perf_counter()
+        with sfft.set_workers(cores):
+            ref = S.zstack(vol, psf, mask=m1, collection_mask=m2)
+        t_cpu = time.perf_counter() - t0
+        extra["cpu_baseline"] = {"value": vol.size / t_cpu, "unit": "voxels/s", "cores": cores, "kind": "port",
+                                 "sample": f"the whole scan by the FP64 SciPy restatement of zstack ({t_cpu:.2f} s)"}
+        err = float(np.linalg.norm(got - ref) / np.linalg.norm(ref))
+        extra["parity"] = {"reference": "oracle restatement of maomi.scanning.zstack (FP64)", "rel_l2": err,
+                           "tolerance": 1e-5, "pass": bool(err < 1e-5)}
+    _line("static scan voxels/s (zstack matlab_convn, 512x512x60 volume, 40x40x46 PSF)", vol.size / (ms * 1e-3),
+          "voxels/s", args, ms,
+          {"workload": "zstack (maomi/scanning.py) of the benchmark volume with the stage's PSF shape and both "
+                       "masks", "transform": [fx, fy], "l2": "spectra 252 MB + kernel spectra 193 MB: above L2"},
+          dtype="f32",
+          e2e={"value": vol.size / (e2e_ms * 1e-3), "unit": "voxels/s",
+               "h2d_bytes_per_step": int(vol.nbytes + psf.nbytes + m1.nbytes + m2.nbytes),
+               "d2h_bytes_per_step": int(vol.nbytes)},
+          gpu_launches=launches,
+          roofline={"bound": "hbm", "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
+                    "frac": achieved / pk["hbm_gbs"], "accounting": "engine passes: each plane read and written "
+                    "once per pass (scan_bytes)", "bytes_per_launch": nbytes, "traffic": None,
+                    "kernel": "plane-convolution engine (all passes)", "peak_source": pk_kind},
+          clocks=clk.summary(), **extra)
+
+
+def run_render(args):
+    """Global cubic-RBF depth render in the configuration of the reference's
+    published renderer timing: a 256 x 256 x 16 fluorescence volume through a
+    3-depth bank of XY-uniform 21 x 21 x 9 excitation kernels
+    (DepthFullFieldRenderer; exact constant-basis reduction per field)."""
+    import torch
+    from maomi_b200 import _lib, synthetic
+    from maomi_b200._scan import transform_size
+    from maomi_b200.rana import DepthFullFieldRenderer, DepthPSFBank, FullFieldPSF
+    dev = "cuda:0"
+    torch.cuda.set_device(0)
+    stream = torch.cuda.current_stream(dev)
+    lib = _lib.load()
+    vol = synthetic.somata_volume((256, 256, 16), count=400, seed=3).astype(np.float64)
+    rng = np.random.default_rng(5)
+    depths = np.array([0.0, 8.0, 16.0])
+    x, y = np.array([0.0, 128.0, 256.0]), np.array([0.0, 128.0, 256.0])
+    g = np.exp(-0.5 * ((np.arange(21) - 10) / 3.0) ** 2)
+    fields = []
+    for d_ in depths:
+        k = (g[:, None, None] * g[None, :, None] * np.exp(-0.5 * ((np.arange(9) - 4) / (2.0 + d_ / 8)) ** 2)[None, None]
+             * rng.uniform(0.95, 1.05, (21, 21, 9)))
+        fields.append(FullFieldPSF(np.broadcast_to(k, (3, 3) + k.shape).copy(), x, y, (1., 1., 1.), 920.,
+                                   "excitation"))
+    bank = DepthPSFBank(depths, tuple(fields))
+    r = DepthFullFieldRenderer(bank, vol.shape, voxel_size_um=(1., 1., 1.), device=dev)
+    src = torch.as_tensor(vol, device=dev)
+    launches0 = lib.mm_launch_count()
+    with Clocks(0) as clk:
+        ms = _timed(lambda: r(src), args.steps, args.warmup, stream)
+    launches = (lib.mm_launch_count() - launches0) / (args.steps + args.warmup)
+    e2e_ms = _timed(lambda: r(vol), args.steps, 1, stream)
+    got = r(vol)
+    f = transform_size(256 + 10)
+    nbytes = len(depths) * scan_bytes(256, 256, 16, 21, 21, 9, f, f, cbytes=16, rbytes=8)
+    pk, pk_kind = peaks()
+    achieved = nbytes / (ms * 1e-3) / 1e9
+    extra = {}
+    if not args.no_cpu_baseline:
+        from oracle import cubic as C
+        t0 = time.perf_counter()
+        ref = C.depth_render(depths, [fl.kernels for fl in fields], x, y, (1., 1., 1.), "excitation", vol)
+        t_cpu = time.perf_counter() - t0
+        extra["cpu_baseline"] = {"value": vol.size / t_cpu, "unit": "voxels/s", "cores": 1, "kind": "port",
+                                 "sample": f"the whole render by the FP64 SciPy restatement ({t_cpu:.2f} s)"}
+        err = float(np.linalg.norm(got - ref) / np.linalg.norm(ref))
+        extra["parity"] = {"reference": "oracle restatement of DepthFullFieldRenderer (FP64)", "rel_l2": err,
+                           "tolerance": 1e-11, "pass": bool(err < 1e-11)}
+    _line("cubic-RBF depth render voxels/s (256x256x16, 3 depths of 21x21x9 kernels)", vol.size / (ms * 1e-3),
+          "voxels/s", args, ms,
+          {"workload": "DepthFullFieldRenderer (maomi/rana/depth.py), excitation, XY-uniform fields (the "
+                       "configuration of the reference's published render timing, 0.0876 s on an RTX 3080)",
+           "transform": [f, f], "l2": "volume 8 MB + spectra 34 MB per field: L2-resident"},
+          dtype="f64",
+          e2e={"value": vol.size / (e2e_ms * 1e-3), "unit": "voxels/s", "h2d_bytes_per_step": int(vol.nbytes),
+               "d2h_bytes_per_step": int(vol.nbytes)},
+          gpu_launches=launches,
+          roofline={"bound": "hbm", "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
+                    "frac": achieved / pk["hbm_gbs"], "accounting": "engine passes (scan_bytes, FP64) per field",
+                    "bytes_per_launch": nbytes, "traffic": None, "kernel": "plane-convolution engine (all passes)",
+                    "peak_source": pk_kind},
+          clocks=clk.summary(), **extra)
+
+
 def run_fields(args):
     """Scattering-field generation for the benchmark geometry: the three raw
     A/B/C fields (768 x 768 x 10/46/4 = 35.4 M voxels), noise drawn on the
@@ -626,7 +775,7 @@ def main():
         return run_reference(args)
     if args.workload != "stage":
         return {"surrogate": run_surrogate, "uneven": run_uneven, "local": run_local,
-                "fields": run_fields}[args.workload](args)
+                "fields": run_fields, "zstack": run_zstack, "render": run_render}[args.workload](args)
     if args.sharded:
         return run_sharded(args)
     import torch

@@ -551,6 +551,11 @@ typedef struct {
   long long o0, o1, o2;
   int accumulate;         /* 1: out += alpha * result; 0: out = alpha * result */
   double alpha;
+  const void* src_spectra;  /* non-NULL: packed source spectra (ceil(planes/2), fx, fy) from mm_scan_forward;
+                               the forward pass is skipped and the spectra are left unchanged */
+  void* out_spectra;        /* non-NULL: stop after the Z rule and store (accumulate 0) or add (1) the packed
+                               output spectra (ceil(out_planes/2), fx, fy) there; `out` is not used */
+  const void* out_weight;   /* non-NULL: (out_x, out_y) row-major weights of the kept window, times alpha */
 } mm_scan_conv;
 
 /* Bytes of a kernel spectrum (kplanes half spectra fx x (fy/2+1), complex). */
@@ -565,6 +570,16 @@ int mm_scan_kernel_spectrum(const mm_scan_desc* desc, const mm_scan_planes* kern
  * scale and store or accumulate. */
 int mm_scan_convolve(const mm_scan_desc* desc, const mm_scan_conv* conv, const void* spectrum, void* workspace,
                      size_t workspace_bytes, void* stream);
+/* Packed spectra (ceil(planes/2), fx, fy) of conv->src (grouping, masks,
+ * wrap as in mm_scan_convolve): a source transformed once and reused by
+ * several mm_scan_convolve calls through conv->src_spectra.  Replaces the
+ * shared source spectrum of CubicFullFieldRenderer.__call__,
+ * maomi/rana/fields.py:248-256. */
+int mm_scan_forward(const mm_scan_desc* desc, const mm_scan_conv* conv, void* spectra, void* stream);
+/* The inverse passes alone: packed spectra (ceil(conv->out_planes/2), fx, fy),
+ * overwritten, to conv->out with its crop, weights, alpha and accumulate
+ * (the final inverse of an accumulated spectrum, maomi/rana/fields.py:265). */
+int mm_scan_inverse(const mm_scan_desc* desc, const mm_scan_conv* conv, void* spectra, void* stream);
 /* The background source plane of blurred_background (movie.py:86-95):
  * out[x,y] = power * mask[x,y] / n * sum_i scale[i] * sum_v vol_v[x,y,idx[i]]
  * over nvol volumes that share one layout (s0, s1, s2); mask may be NULL.

@@ -79,7 +79,8 @@ class ScanConv(Structure):
     _fields_ = [("src", ScanPlanes), ("wrap", c_int), ("wrap_x0", c_int), ("wrap_y0", c_int), ("ext_x", c_int),
                 ("ext_y", c_int), ("zrule", c_int), ("zoff", c_int), ("out_planes", c_int), ("crop_x", c_int),
                 ("crop_y", c_int), ("out_x", c_int), ("out_y", c_int), ("out", c_void_p), ("o0", ctypes.c_longlong),
-                ("o1", ctypes.c_longlong), ("o2", ctypes.c_longlong), ("accumulate", c_int), ("alpha", c_double)]
+                ("o1", ctypes.c_longlong), ("o2", ctypes.c_longlong), ("accumulate", c_int), ("alpha", c_double),
+                ("src_spectra", c_void_p), ("out_spectra", c_void_p), ("out_weight", c_void_p)]
 
 
 MM_SCAN_CONV_Z, MM_SCAN_CORR_Z, MM_SCAN_SUM_Z, MM_SCAN_EACH_Z = 0, 1, 2, 3
@@ -155,6 +156,8 @@ SIGNATURES = {
     "mm_scan_kernel_spectrum": (c_int, [POINTER(ScanDesc), POINTER(ScanPlanes), c_void_p, c_void_p, c_size_t,
                                         c_void_p]),
     "mm_scan_convolve": (c_int, [POINTER(ScanDesc), POINTER(ScanConv), c_void_p, c_void_p, c_size_t, c_void_p]),
+    "mm_scan_forward": (c_int, [POINTER(ScanDesc), POINTER(ScanConv), c_void_p, c_void_p]),
+    "mm_scan_inverse": (c_int, [POINTER(ScanDesc), POINTER(ScanConv), c_void_p, c_void_p]),
     "mm_scan_background": (c_int, [c_int, POINTER(c_void_p), c_int, ctypes.c_longlong, ctypes.c_longlong,
                                    ctypes.c_longlong, c_int, c_int, c_int, c_void_p, c_void_p, c_int, c_double,
                                    c_void_p, c_void_p, c_void_p]),

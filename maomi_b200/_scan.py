@@ -77,25 +77,72 @@ class KernelSpectrum:
         self._keep = kernel  # the kernel stays alive until the stream has read it
 
     def convolve(self, src, *, zrule, out, crop, out_shape, out_planes, zoff=0, group=1, masks=(None, None),
-                 wrap=None, accumulate=False, alpha=1.0):
-        """One engine pass of ``src`` (3-D device tensor) into ``out``."""
+                 wrap=None, accumulate=False, alpha=1.0, src_spectra=None, out_spectra=None, out_weight=None):
+        """One engine pass of ``src`` (3-D device tensor) into ``out``.
+
+        ``src_spectra``: the source's packed spectra (``forward_spectra``),
+        reused instead of transforming ``src`` again; ``out_spectra``: store
+        (or, with ``accumulate``, add) the packed output spectra there and
+        skip the inverse; ``out_weight``: (out_x, out_y) weights of the kept
+        window."""
         lib = _lib.load()
-        if src.dtype != self.dtype or out.dtype != self.dtype:
+        if src.dtype != self.dtype or (out is not None and out.dtype != self.dtype):
             raise ValueError("source, kernel and output must share one floating type")
         rec = planes_record(src, group=group, masks=masks)
         nin = -(-int(src.shape[2]) // int(group))
-        if wrap is None:
-            wrap_flag, wx0, wy0, ext_x, ext_y = 0, 0, 0, int(src.shape[0]), int(src.shape[1])
-        else:
-            wrap_flag, (wx0, wy0), (ext_x, ext_y) = 1, wrap[0], wrap[1]
-        o = out.stride() if out.dim() == 3 else (out.stride(0), out.stride(1), 0)
-        conv = _lib.ScanConv(rec, wrap_flag, int(wx0), int(wy0), int(ext_x), int(ext_y), int(zrule), int(zoff),
-                             int(out_planes), int(crop[0]), int(crop[1]), int(out_shape[0]), int(out_shape[1]),
-                             out.data_ptr(), o[0], o[1], o[2], int(bool(accumulate)), float(alpha))
-        work = workspace(self.desc, max(nin, int(out_planes)), self.device)
+        conv = conv_record(src, rec, wrap, zrule, zoff, out_planes, crop, out_shape, out, accumulate, alpha)
+        conv.src_spectra = None if src_spectra is None else src_spectra.data_ptr()
+        conv.out_spectra = None if out_spectra is None else out_spectra.data_ptr()
+        conv.out_weight = None if out_weight is None else out_weight.data_ptr()
+        planes = 0 if (src_spectra is not None and out_spectra is not None) else (
+            int(out_planes) if src_spectra is not None else max(nin, int(out_planes)))
+        work = workspace(self.desc, planes, self.device) if planes else None
         _lib.check(lib.mm_scan_convolve(ctypes.byref(self.desc), ctypes.byref(conv), _lib.ptr(self.data),
-                                        _lib.ptr(work), work.numel(), _lib.stream_of(self.device)), "plane convolution")
+                                        _lib.ptr(work), 0 if work is None else work.numel(),
+                                        _lib.stream_of(self.device)), "plane convolution")
         return out
+
+
+def conv_record(src, rec, wrap, zrule, zoff, out_planes, crop, out_shape, out, accumulate, alpha):
+    if wrap is None:
+        wrap_flag, wx0, wy0, ext_x, ext_y = 0, 0, 0, int(src.shape[0]), int(src.shape[1])
+    else:
+        wrap_flag, (wx0, wy0), (ext_x, ext_y) = 1, wrap[0], wrap[1]
+    if out is None:
+        ptr, o = None, (0, 0, 0)
+    else:
+        ptr, o = out.data_ptr(), (out.stride() if out.dim() == 3 else (out.stride(0), out.stride(1), 0))
+    return _lib.ScanConv(rec, wrap_flag, int(wx0), int(wy0), int(ext_x), int(ext_y), int(zrule), int(zoff),
+                         int(out_planes), int(crop[0]), int(crop[1]), int(out_shape[0]), int(out_shape[1]), ptr,
+                         o[0], o[1], o[2], int(bool(accumulate)), float(alpha))
+
+
+def spectra_buffer(desc, planes, device):
+    """Packed spectra of ``planes`` transform planes (complex pairs, fx x fy)."""
+    return workspace(desc, planes, device)
+
+
+def forward_spectra(desc, src, *, masks=(None, None), group=1):
+    """Packed spectra of the planes of ``src`` at the transform sizes of ``desc``."""
+    planes = -(-int(src.shape[2]) // int(group))
+    buf = spectra_buffer(desc, planes, src.device)
+    rec = planes_record(src, group=group, masks=masks)
+    conv = conv_record(src, rec, None, 0, 0, planes, (0, 0), (1, 1), None, False, 1.0)
+    _lib.check(_lib.load().mm_scan_forward(ctypes.byref(desc), ctypes.byref(conv), _lib.ptr(buf),
+                                           _lib.stream_of(src.device)), "plane transform")
+    return buf
+
+
+def inverse_spectra(desc, spectra, out, *, crop, out_shape, out_planes, accumulate=False, alpha=1.0,
+                    out_weight=None):
+    """Inverse passes of packed spectra (overwritten) into ``out``."""
+    dummy = out if out.dim() == 3 else out[..., None]
+    rec = planes_record(dummy)
+    conv = conv_record(dummy, rec, None, 0, 0, out_planes, crop, out_shape, out, accumulate, alpha)
+    conv.out_weight = None if out_weight is None else out_weight.data_ptr()
+    _lib.check(_lib.load().mm_scan_inverse(ctypes.byref(desc), ctypes.byref(conv), _lib.ptr(spectra),
+                                           _lib.stream_of(out.device)), "inverse plane transform")
+    return out
 
 
 def workspace(desc, planes, device):

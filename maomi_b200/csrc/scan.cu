@@ -237,13 +237,15 @@ __device__ __forceinline__ void hsplit(C w, C wm, C& a, C& b) {
 
 // Bin pair representative: ky in [0, fy/2]; on the self-paired columns
 // (ky = 0, fy/2) only kx in [0, fx/2].  One thread per representative.
-// Source spectra S (pairs_in, fx, fy) are overwritten with the output
-// spectra (pairs_out, fx, fy): a thread reads its two bins of every plane
-// before writing them.  Kernel half spectra K (nk, fx, fy/2 + 1).
+// Source spectra Sin (pairs_in, fx, fy) -> output spectra S (pairs_out, fx,
+// fy), stored or (accumulate) added.  S may be Sin: a thread reads its two
+// bins of every source plane before it writes any output bin.  Kernel half
+// spectra K (nk, fx, fy/2 + 1).
 template <class T>
-__global__ void __launch_bounds__(kCombineThreads) combine_kernel(typename Cplx<T>::type* __restrict__ S,
+__global__ void __launch_bounds__(kCombineThreads) combine_kernel(const typename Cplx<T>::type* Sin,
+                                                                  typename Cplx<T>::type* S,
                                                                   const typename Cplx<T>::type* __restrict__ K,
-                                                                  int fx, int fy, Rule R, T scale) {
+                                                                  int fx, int fy, Rule R, T scale, int accumulate) {
   using C = typename Cplx<T>::type;
   extern __shared__ __align__(16) unsigned char smem[];
   C* sv = reinterpret_cast<C*>(smem);  // (nin, blockDim) source bins of this thread
@@ -261,7 +263,7 @@ __global__ void __launch_bounds__(kCombineThreads) combine_kernel(typename Cplx<
   const int pin = (R.nin + 1) / 2;
   for (int p = 0; p < pin; ++p) {
     C a, bb;
-    hsplit(S[p * plane + ik], S[p * plane + im], a, bb);
+    hsplit(Sin[p * plane + ik], Sin[p * plane + im], a, bb);
     sv[(2 * p) * nt + tid] = a;
     if (2 * p + 1 < R.nin) sv[(2 * p + 1) * nt + tid] = bb;
   }
@@ -269,37 +271,73 @@ __global__ void __launch_bounds__(kCombineThreads) combine_kernel(typename Cplx<
   const long long kplane = (long long)fx * hy;
   const int pout = (R.nout + 1) / 2;
   const C zero = make_c<C>(0.0, 0.0);
-  for (int q = 0; q < pout; ++q) {
-    C y[2] = {zero, zero};
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const int o = 2 * q + h;
-      if (o >= R.nout) break;
-      C acc = zero;
-      if (R.zrule == MM_SCAN_SUM_Z) {
-        for (int z = 0; z < R.nin; ++z) acc = cadd(acc, cmul(sv[z * nt + tid], kk[z * kplane]));
-      } else if (R.zrule == MM_SCAN_EACH_Z) {
-        acc = cmul(sv[o * nt + tid], kk[o * kplane]);
-      } else {
-        // CONV: z = o + zoff - l;  CORR: z = o - zoff + l
-        const bool conv = R.zrule == MM_SCAN_CONV_Z;
-        const int lo = conv ? max(0, o + R.zoff - (R.nin - 1)) : max(0, R.zoff - o);
-        const int hi = conv ? min(R.nk - 1, o + R.zoff) : min(R.nk - 1, R.nin - 1 - o + R.zoff);
-        for (int l = lo; l <= hi; ++l) {
-          const int z = conv ? o + R.zoff - l : o - R.zoff + l;
-          acc = cadd(acc, cmul(sv[z * nt + tid], kk[l * kplane]));
-        }
-      }
-      y[h] = make_c<C>(acc.x * scale, acc.y * scale);
-    }
-    // packed output: W(k) = Y0(k) + i Y1(k);  W(-k) = conj(Y0(k)) + i conj(Y1(k))
+  // packed output: W(k) = Y0(k) + i Y1(k);  W(-k) = conj(Y0(k)) + i conj(Y1(k))
+  auto store = [&](int q, C y0, C y1) {
     C wk, wm;
-    wk.x = y[0].x - y[1].y;
-    wk.y = y[0].y + y[1].x;
-    wm.x = y[0].x + y[1].y;
-    wm.y = y[1].x - y[0].y;
+    wk.x = y0.x - y1.y;
+    wk.y = y0.y + y1.x;
+    wm.x = y0.x + y1.y;
+    wm.y = y1.x - y0.y;
+    if (accumulate) {
+      wk = cadd(S[q * plane + ik], wk);
+      if (!self) wm = cadd(S[q * plane + im], wm);
+    }
     S[q * plane + ik] = wk;
     if (!self) S[q * plane + im] = wm;
+  };
+  auto scaled = [&](C a) { return make_c<C>(a.x * scale, a.y * scale); };
+  if (R.zrule == MM_SCAN_SUM_Z || R.zrule == MM_SCAN_EACH_Z) {
+    for (int q = 0; q < pout; ++q) {
+      C y[2] = {zero, zero};
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int o = 2 * q + h;
+        if (o >= R.nout) break;
+        C acc = zero;
+        if (R.zrule == MM_SCAN_SUM_Z) {
+          for (int z = 0; z < R.nin; ++z) acc = cadd(acc, cmul(sv[z * nt + tid], kk[z * kplane]));
+        } else {
+          acc = cmul(sv[o * nt + tid], kk[o * kplane]);
+        }
+        y[h] = scaled(acc);
+      }
+      store(q, y[0], y[1]);
+    }
+    return;
+  }
+  // CONV: z = o + zoff - l;  CORR: z = o - zoff + l.  Outputs in register
+  // chunks of kOutChunk: each kernel bin is read once per chunk, every
+  // output still sums its taps in increasing l.
+  constexpr int kOutChunk = 16;
+  const bool conv = R.zrule == MM_SCAN_CONV_Z;
+  for (int o0 = 0; o0 < R.nout; o0 += kOutChunk) {
+    C y[kOutChunk];
+#pragma unroll
+    for (int j = 0; j < kOutChunk; ++j) y[j] = zero;
+    const int oe = min(o0 + kOutChunk, R.nout) - 1;
+    const int lo = conv ? max(0, o0 + R.zoff - (R.nin - 1)) : max(0, R.zoff - oe);
+    const int hi = conv ? min(R.nk - 1, oe + R.zoff) : min(R.nk - 1, R.nin - 1 - o0 + R.zoff);
+    for (int l = lo; l <= hi; ++l) {
+      const C kl = kk[l * kplane];
+      const int z0 = conv ? o0 + R.zoff - l : o0 - R.zoff + l;  // source plane of output o0
+      if (z0 >= 0 && z0 + kOutChunk <= R.nin && o0 + kOutChunk - 1 <= oe) {
+        // interior: every output of the chunk reads a source plane
+        const C* vp = sv + (long long)z0 * nt + tid;
+#pragma unroll
+        for (int j = 0; j < kOutChunk; ++j) y[j] = cadd(y[j], cmul(vp[j * nt], kl));
+      } else {
+#pragma unroll
+        for (int j = 0; j < kOutChunk; ++j) {
+          const int z = z0 + j;
+          if (o0 + j <= oe && z >= 0 && z < R.nin) y[j] = cadd(y[j], cmul(sv[z * nt + tid], kl));
+        }
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < kOutChunk; j += 2) {
+      if (o0 + j > oe) break;
+      store((o0 + j) / 2, scaled(y[j]), o0 + j + 1 <= oe ? scaled(y[j + 1]) : zero);
+    }
   }
 }
 
@@ -334,6 +372,7 @@ struct Out {
   long long o0, o1, o2;
   int out_x, out_y, planes, crop_y, accumulate;
   double alpha;
+  const void* weight;  // (out_x, out_y) row-major weights of the kept window, or NULL
 };
 
 template <class T, int N>
@@ -374,13 +413,15 @@ __global__ void __launch_bounds__(kThreads) rows_inv_kernel(const typename Cplx<
   const bool pfast = O.o2 < O.o1;
   T* out = static_cast<T*>(O.data);
   const T alpha = T(O.alpha);
+  const T* wrow = O.weight ? static_cast<const T*>(O.weight) + (long long)r * O.out_y : nullptr;
   const int total = O.out_y * np;
   for (int e = threadIdx.x; e < total; e += kThreads) {
     int j, q;
     if (pfast) { j = e / np; q = e - j * np; }
     else { q = e / O.out_y; j = e - q * O.out_y; }
     const long long a = (long long)r * O.o0 + (long long)j * O.o1 + (long long)(p0 + q) * O.o2;
-    const T val = alpha * tile[j * TP + q];
+    T val = alpha * tile[j * TP + q];
+    if (wrow) val *= wrow[j];
     out[a] = O.accumulate ? out[a] + val : val;
   }
 }
@@ -553,13 +594,43 @@ int kernel_spectrum(const mm_scan_desc* d, const mm_scan_planes* k, void* spectr
   return MM_OK;
 }
 
+// Inverse passes of packed spectra S (overwritten): columns keeping the crop
+// rows, rows keeping the crop columns, unpacked, weighted, scaled, stored.
+template <class T>
+int inverse(const mm_scan_desc* d, const mm_scan_conv* c, int planes, void* S, cudaStream_t st) {
+  MM_CHECK_ARG(c->out != nullptr, "scan: null output");
+  MM_CHECK_ARG(c->out_x >= 1 && c->out_y >= 1 && c->crop_x >= 0 && c->crop_y >= 0 &&
+                   c->crop_x + c->out_x <= d->fx && c->crop_y + c->out_y <= d->fy,
+               "scan: kept window [%d, %d) x [%d, %d) outside the transform %d x %d", c->crop_x, c->crop_x + c->out_x,
+               c->crop_y, c->crop_y + c->out_y, d->fx, d->fy);
+  const int pairs = (planes + 1) / 2;
+  int rc = by_size<T>(d->fx, [&](auto n) {
+    return cols<T, decltype(n)::value, +1>(S, d->fy, pairs, d->fx, c->crop_x, c->out_x, st);
+  });
+  if (rc) return rc;
+  Out O;
+  O.data = c->out;
+  O.o0 = c->o0;
+  O.o1 = c->o1;
+  O.o2 = c->o2;
+  O.out_x = c->out_x;
+  O.out_y = c->out_y;
+  O.planes = planes;
+  O.crop_y = c->crop_y;
+  O.accumulate = c->accumulate;
+  O.alpha = c->alpha;
+  O.weight = c->out_weight;
+  return by_size<T>(d->fy, [&](auto n) { return rows_inv<T, decltype(n)::value>(S, d->fx, O, st); });
+}
+
 template <class T>
 int convolve(const mm_scan_desc* d, const mm_scan_conv* c, const void* spectrum, void* work, size_t wbytes,
              cudaStream_t st) {
   using C = typename Cplx<T>::type;
   int rc = check_planes(&c->src, d->fx, d->fy, c->ext_x, c->ext_y);
   if (rc) return rc;
-  MM_CHECK_ARG(spectrum != nullptr && c->out != nullptr, "scan: null spectrum or output");
+  MM_CHECK_ARG(spectrum != nullptr && (c->out != nullptr || c->out_spectra != nullptr),
+               "scan: null spectrum or output");
   Planes P = make_planes(&c->src, c->wrap, c->wrap_x0, c->wrap_y0, c->ext_x, c->ext_y);
   MM_CHECK_ARG(!c->wrap || (c->wrap_x0 >= 0 && c->wrap_y0 >= 0), "scan: wrap offsets must be nonnegative");
   Rule R;
@@ -585,48 +656,38 @@ int convolve(const mm_scan_desc* d, const mm_scan_conv* c, const void* spectrum,
     default:
       MM_CHECK_ARG(false, "scan: unknown Z rule %d", c->zrule);
   }
-  MM_CHECK_ARG(c->out_x >= 1 && c->out_y >= 1 && c->crop_x >= 0 && c->crop_y >= 0 &&
-                   c->crop_x + c->out_x <= d->fx && c->crop_y + c->out_y <= d->fy,
-               "scan: kept window [%d, %d) x [%d, %d) outside the transform %d x %d", c->crop_x, c->crop_x + c->out_x,
-               c->crop_y, c->crop_y + c->out_y, d->fx, d->fy);
   // alias-free: the linear convolution's support ends at ext + k - 1
   MM_CHECK_ARG(c->ext_x + d->kx - 1 <= d->fx + c->crop_x && c->ext_y + d->ky - 1 <= d->fy + c->crop_y,
                "scan: transform %d x %d too small for inputs %d x %d and kernels %d x %d at crop (%d, %d)", d->fx,
                d->fy, c->ext_x, c->ext_y, d->kx, d->ky, c->crop_x, c->crop_y);
-  const int pairs_in = (R.nin + 1) / 2, pairs_out = (R.nout + 1) / 2;
-  const size_t need = mm_scan_workspace_size(d, std::max(R.nin, R.nout));
-  MM_CHECK_ARG(work != nullptr && wbytes >= need, "scan: workspace of %zu bytes needed", need);
+  const int pairs_out = (R.nout + 1) / 2;
+  // workspace: the source spectra (unless given) and the output spectra
+  // (unless stored elsewhere)
+  const int wplanes = c->src_spectra ? (c->out_spectra ? 0 : R.nout) : std::max(R.nin, R.nout);
+  const size_t need = wplanes ? mm_scan_workspace_size(d, wplanes) : 0;
+  MM_CHECK_ARG(!need || (work != nullptr && wbytes >= need), "scan: workspace of %zu bytes needed", need);
   // combine: per-thread source bins in shared memory
   int threads = kCombineThreads;
   while (threads > 32 && (size_t)R.nin * threads * sizeof(C) > 200 * 1024) threads /= 2;
   const size_t csmem = (size_t)R.nin * threads * sizeof(C);
   MM_CHECK_ARG(csmem <= 200 * 1024, "scan: %d source planes exceed the combine kernel's shared memory", R.nin);
-  rc = forward<T>(P, d->fx, d->fy, work, st);
-  if (rc) return rc;
-  (void)pairs_in;
+  const C* sin = static_cast<const C*>(c->src_spectra);
+  if (!sin) {
+    rc = forward<T>(P, d->fx, d->fy, work, st);
+    if (rc) return rc;
+    sin = static_cast<const C*>(work);
+  }
+  C* sout = c->out_spectra ? static_cast<C*>(c->out_spectra) : static_cast<C*>(work);
   MM_CHECK_CUDA(cudaFuncSetAttribute(combine_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csmem),
                 "cudaFuncSetAttribute(scan combine)");
   const long long bins = (long long)d->fx * (d->fy / 2 + 1);
   const T scale = T(1.0 / (double(d->fx) * double(d->fy)));
   combine_kernel<T><<<(unsigned)((bins + threads - 1) / threads), threads, csmem, st>>>(
-      static_cast<C*>(work), static_cast<const C*>(spectrum), d->fx, d->fy, R, scale);
+      sin, sout, static_cast<const C*>(spectrum), d->fx, d->fy, R, scale, c->out_spectra ? c->accumulate : 0);
   MM_CHECK_LAUNCH("scan combine");
-  rc = by_size<T>(d->fx, [&](auto n) {
-    return cols<T, decltype(n)::value, +1>(work, d->fy, pairs_out, d->fx, c->crop_x, c->out_x, st);
-  });
-  if (rc) return rc;
-  Out O;
-  O.data = c->out;
-  O.o0 = c->o0;
-  O.o1 = c->o1;
-  O.o2 = c->o2;
-  O.out_x = c->out_x;
-  O.out_y = c->out_y;
-  O.planes = R.nout;
-  O.crop_y = c->crop_y;
-  O.accumulate = c->accumulate;
-  O.alpha = c->alpha;
-  return by_size<T>(d->fy, [&](auto n) { return rows_inv<T, decltype(n)::value>(work, d->fx, O, st); });
+  if (c->out_spectra) return MM_OK;
+  return inverse<T>(d, c, R.nout, sout, st);
+  (void)pairs_out;
 }
 
 }  // namespace scan
@@ -663,6 +724,27 @@ extern "C" int mm_scan_convolve(const mm_scan_desc* d, const mm_scan_conv* c, co
   auto st = static_cast<cudaStream_t>(stream);
   return d->fp64 ? scan::convolve<double>(d, c, spectrum, work, wbytes, st)
                  : scan::convolve<float>(d, c, spectrum, work, wbytes, st);
+}
+
+extern "C" int mm_scan_forward(const mm_scan_desc* d, const mm_scan_conv* c, void* spectra, void* stream) {
+  int rc = scan::check_desc(d);
+  if (rc) return rc;
+  MM_CHECK_ARG(c != nullptr && spectra != nullptr, "scan: null convolution or spectra");
+  rc = scan::check_planes(&c->src, d->fx, d->fy, c->ext_x, c->ext_y);
+  if (rc) return rc;
+  MM_CHECK_ARG(!c->wrap || (c->wrap_x0 >= 0 && c->wrap_y0 >= 0), "scan: wrap offsets must be nonnegative");
+  scan::Planes P = scan::make_planes(&c->src, c->wrap, c->wrap_x0, c->wrap_y0, c->ext_x, c->ext_y);
+  auto st = static_cast<cudaStream_t>(stream);
+  return d->fp64 ? scan::forward<double>(P, d->fx, d->fy, spectra, st) : scan::forward<float>(P, d->fx, d->fy, spectra, st);
+}
+
+extern "C" int mm_scan_inverse(const mm_scan_desc* d, const mm_scan_conv* c, void* spectra, void* stream) {
+  int rc = scan::check_desc(d);
+  if (rc) return rc;
+  MM_CHECK_ARG(c != nullptr && spectra != nullptr && c->out_planes >= 1, "scan: bad inverse arguments");
+  auto st = static_cast<cudaStream_t>(stream);
+  return d->fp64 ? scan::inverse<double>(d, c, c->out_planes, spectra, st)
+                 : scan::inverse<float>(d, c, c->out_planes, spectra, st);
 }
 
 extern "C" int mm_scan_background(int fp64, const void* const* volumes, int nvol, long long s0, long long s1,

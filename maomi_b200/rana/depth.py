@@ -103,3 +103,55 @@ class DepthPSFBank:
                                  f"{len(meta)} provenance records")
             common = (d["x_um"], d["y_um"], tuple(d["voxel_size_um"]), float(d["wavelength_nm"]), str(d["operator"]))
             return cls(d["depths_um"], tuple(FullFieldPSF(k, *common, m) for k, m in zip(d["kernels"], meta)))
+
+
+class DepthFullFieldRenderer:
+    """Cubic XY fields with linear focal-depth weights (maomi/rana/depth.py:72-104).
+
+    One ``CubicFullFieldRenderer`` per depth field; detection weights the
+    source planes before the convolution, excitation weights the image planes
+    after the correlation.  The depth sum runs on the device; fields whose
+    depth weights are all zero are skipped."""
+
+    def __init__(self, bank, shape, *, voxel_size_um, origin_um=(0., 0.), z_origin_um=0., device="cuda"):
+        from .cubic import CubicFullFieldRenderer
+        if not isinstance(bank, DepthPSFBank) or len(shape) != 3:
+            raise TypeError("Depth rendering requires DepthPSFBank and an XYZ volume")
+        if not np.isfinite(z_origin_um):
+            raise ValueError("z_origin_um must be finite")
+        end = z_origin_um + shape[2] * voxel_size_um[2]
+        if z_origin_um < bank.depths_um[0] or end > bank.depths_um[-1]:
+            raise ValueError("Depth bank must cover the entire Z extent including edges")
+        self.bank, self.shape = bank, tuple(shape)
+        z = z_origin_um + (np.arange(shape[2]) + .5) * voxel_size_um[2]
+        self.weights = depth_weights(bank.depths_um, z)
+        self.renderers = [CubicFullFieldRenderer(f, shape, voxel_size_um=voxel_size_um, origin_um=origin_um,
+                                                 device=device) for f in bank.fields]
+        self.device = self.renderers[0].device
+        self.validation = {"depth_nodes_um": bank.depths_um.tolist(), "checked_xyz_positions": int(np.prod(shape)),
+                           "shared_psf_fallback": False, "depth_interpolation": "positive linear",
+                           "fields": [r.validation for r in self.renderers]}
+
+    def __call__(self, density):
+        import torch
+        from .. import _lib
+        src = (density.to(device=self.device, dtype=torch.float64) if isinstance(density, torch.Tensor)
+               else _lib.upload(np.asarray(density, dtype=float), self.device))
+        result = torch.zeros(self.shape, dtype=torch.float64, device=self.device)
+        for w, renderer in zip(self.weights, self.renderers):
+            if not np.any(w):
+                continue
+            wd = torch.as_tensor(w, dtype=torch.float64, device=self.device)[None, None, :]
+            if self.bank.operator == "detection":
+                result += _checked(renderer, src * wd)
+            else:
+                result += _checked(renderer, src) * wd
+        return result.cpu().numpy()
+
+
+def _checked(renderer, src):
+    """One field's image with the single-field renderer's input and output checks."""
+    import torch
+    if (tuple(src.shape) != renderer.shape or not bool(torch.isfinite(src).all()) or bool((src < 0).any())):
+        raise ValueError("Density must be finite, nonnegative and match the prepared shape")
+    return renderer.render_device(src)

@@ -411,10 +411,77 @@ def make_collection(torch):
     return out
 
 
+def make_cubic(torch):
+    """The reference's global cubic-RBF renderers on seeded fields:
+    ``CubicFullFieldRenderer`` (maomi/rana/fields.py:113-276) for 2-D and 3-D
+    shapes, both operators, even and odd kernels, a non-affine knot and a
+    16 x 16-node field; ``DepthFullFieldRenderer`` (maomi/rana/depth.py:72-104)
+    with uniform and varying XY fields."""
+    from maomi.rana.depth import DepthFullFieldRenderer, DepthPSFBank
+    from maomi.rana.fields import CubicFullFieldRenderer, FullFieldPSF
+    out = {}
+    rng = np.random.default_rng(47)
+    case = 0
+    for shape in [(5, 4), (4, 3, 3)]:
+        for kshape in [(3,) * len(shape), (4, 2) + ((2,) if len(shape) == 3 else ())]:
+            for op in ("detection", "excitation"):
+                r = np.random.default_rng(18)
+                base, dx, dy = r.uniform(.2, 1, kshape), r.uniform(0, .5, kshape), r.uniform(0, .4, kshape)
+                x, y = np.linspace(0, shape[0], 3), np.linspace(0, shape[1], 3)
+                k = np.array([[base + xx / shape[0] * dx + yy / shape[1] * dy for yy in y] for xx in x])
+                a = rng.uniform(0, 2, shape)
+                f = FullFieldPSF(k, x, y, (1.,) * len(shape), 920., op)
+                out.update({f"k{case}_kernels": k, f"k{case}_x": x, f"k{case}_y": y, f"k{case}_density": a,
+                            f"k{case}_op": np.asarray(op),
+                            f"k{case}_image": CubicFullFieldRenderer(f, shape, voxel_size_um=(1,) * len(shape))(a)})
+                case += 1
+    # non-affine knot, and a 16 x 16-node varying field with an origin offset
+    k = out["k0_kernels"].copy()
+    k[1, 1] *= 1.15
+    a = np.random.default_rng(12).uniform(0, 1, (5, 4))
+    f = FullFieldPSF(k, out["k0_x"], out["k0_y"], (1, 1), 920, "detection")
+    out.update({f"k{case}_kernels": k, f"k{case}_x": out["k0_x"], f"k{case}_y": out["k0_y"], f"k{case}_density": a,
+                f"k{case}_op": np.asarray("detection"),
+                f"k{case}_image": CubicFullFieldRenderer(f, (5, 4), voxel_size_um=(1, 1))(a)})
+    case += 1
+    r = np.random.default_rng(33)
+    x, y = np.linspace(0, 48, 16) + 2.0, np.linspace(0, 40, 16) - 1.0
+    base = r.uniform(.5, 1, (7, 7, 3))
+    k = np.array([[base * (1 + .2 * np.sin(xx / 9) * np.cos(yy / 7)) + .05 * r.uniform(0, 1, base.shape)
+                   for yy in y] for xx in x])
+    for op in ("detection", "excitation"):
+        a = r.uniform(0, 1, (48, 40, 6))
+        f = FullFieldPSF(k, x, y, (1., 1., 1.), 920., op)
+        img = CubicFullFieldRenderer(f, a.shape, voxel_size_um=(1, 1, 1), origin_um=(2.0, -1.0))(a)
+        out.update({f"k{case}_kernels": k, f"k{case}_x": x, f"k{case}_y": y, f"k{case}_density": a,
+                    f"k{case}_op": np.asarray(op), f"k{case}_origin": np.array([2.0, -1.0]), f"k{case}_image": img})
+        case += 1
+    out["cases"] = np.asarray(case)
+    # depth banks: uniform XY (exact constant basis) and varying XY
+    depths = np.array([0.0, 3.0, 8.0])
+    for name, vary in (("uniform", False), ("varying", True)):
+        for op in ("detection", "excitation"):
+            r = np.random.default_rng(71)
+            x, y = np.array([0.0, 12.0, 24.0]), np.array([0.0, 10.0, 20.0])
+            kern = []
+            for d in depths:
+                b = r.uniform(.3, 1, (5, 5, 3)) * (1 + d / 10)
+                kern.append(np.array([[b * ((1 + .1 * xx / 24 + .05 * yy / 20) if vary else 1) for yy in y]
+                                      for xx in x]))
+            bank = DepthPSFBank(depths, tuple(FullFieldPSF(kk, x, y, (1., 1., 1.), 920., op) for kk in kern))
+            a = r.uniform(0, 1, (24, 20, 8))
+            img = DepthFullFieldRenderer(bank, a.shape, voxel_size_um=(1., 1., 1.))(a)
+            out.update({f"d_{name}_{op}_kernels": np.stack(kern), f"d_{name}_{op}_density": a,
+                        f"d_{name}_{op}_image": img})
+    out.update(d_depths=depths, d_x=np.array([0.0, 12.0, 24.0]), d_y=np.array([0.0, 10.0, 20.0]))
+    return out
+
+
 MAKERS = (("numerics", make_numerics), ("local_fft", make_local_fft), ("stage_small", make_stage_small),
           ("stage_reftest", make_stage_reftest), ("stage_bench_sites", make_stage_bench_sites),
           ("fields", make_fields), ("stage_bench_lattice", make_stage_bench_lattice), ("rana_files", make_rana_files),
-          ("scanning", make_scanning), ("collection", make_collection))
+          ("scanning", make_scanning), ("collection", make_collection),
+          ("cubic", make_cubic))
 
 
 def main(ref_path, only=None):
