@@ -235,6 +235,37 @@ __device__ __forceinline__ void hsplit(C w, C wm, C& a, C& b) {
   b.y = (wm.x - w.x) * 0.5f;
 }
 
+// CONV / CORR rule for one chunk of kOutChunk outputs with register windows
+// (FP32): 16 taps at a time, the 31 source bins they reach read once from
+// shared memory and the 16 kernel bins once from global memory; terms outside
+// the source or kernel range are exact zeros, so every output sums its taps
+// in increasing l exactly as the one-tap loop does.
+constexpr int kOutChunk = 16;
+
+template <bool CONV, class C>
+__device__ __forceinline__ void zrule_window(C (&y)[kOutChunk], const C* sv, int nt, int tid, const C* kk,
+                                             long long kplane, int o0, int zoff, int lo, int hi, int nin) {
+  constexpr int TB = 16;
+  const C zero = make_c<C>(0.0, 0.0);
+  for (int l0 = lo; l0 <= hi; l0 += TB) {
+    C kb[TB];
+#pragma unroll
+    for (int ll = 0; ll < TB; ++ll) kb[ll] = (l0 + ll <= hi) ? kk[(long long)(l0 + ll) * kplane] : zero;
+    // CONV: z = o0 + j + zoff - l0 - ll = zb + (TB - 1) + j - ll;  CORR: z = zb + j + ll
+    const int zb = CONV ? o0 + zoff - l0 - (TB - 1) : o0 - zoff + l0;
+    C w[2 * TB - 1];
+#pragma unroll
+    for (int i = 0; i < 2 * TB - 1; ++i) {
+      const int z = zb + i;
+      w[i] = (z >= 0 && z < nin) ? sv[z * nt + tid] : zero;
+    }
+#pragma unroll
+    for (int ll = 0; ll < TB; ++ll)
+#pragma unroll
+      for (int j = 0; j < kOutChunk; ++j) y[j] = cadd(y[j], cmul(w[CONV ? j - ll + TB - 1 : j + ll], kb[ll]));
+  }
+}
+
 // Bin pair representative: ky in [0, fy/2]; on the self-paired columns
 // (ky = 0, fy/2) only kx in [0, fx/2].  One thread per representative.
 // Source spectra Sin (pairs_in, fx, fy) -> output spectra S (pairs_out, fx,
@@ -308,7 +339,6 @@ __global__ void __launch_bounds__(kCombineThreads) combine_kernel(const typename
   // CONV: z = o + zoff - l;  CORR: z = o - zoff + l.  Outputs in register
   // chunks of kOutChunk: each kernel bin is read once per chunk, every
   // output still sums its taps in increasing l.
-  constexpr int kOutChunk = 16;
   const bool conv = R.zrule == MM_SCAN_CONV_Z;
   for (int o0 = 0; o0 < R.nout; o0 += kOutChunk) {
     C y[kOutChunk];
@@ -317,6 +347,10 @@ __global__ void __launch_bounds__(kCombineThreads) combine_kernel(const typename
     const int oe = min(o0 + kOutChunk, R.nout) - 1;
     const int lo = conv ? max(0, o0 + R.zoff - (R.nin - 1)) : max(0, R.zoff - oe);
     const int hi = conv ? min(R.nk - 1, oe + R.zoff) : min(R.nk - 1, R.nin - 1 - o0 + R.zoff);
+    if constexpr (std::is_same_v<T, float>) {
+      if (conv) zrule_window<true>(y, sv, nt, tid, kk, kplane, o0, R.zoff, lo, hi, R.nin);
+      else zrule_window<false>(y, sv, nt, tid, kk, kplane, o0, R.zoff, lo, hi, R.nin);
+    } else {
     for (int l = lo; l <= hi; ++l) {
       const C kl = kk[l * kplane];
       const int z0 = conv ? o0 + R.zoff - l : o0 - R.zoff + l;  // source plane of output o0
@@ -332,6 +366,7 @@ __global__ void __launch_bounds__(kCombineThreads) combine_kernel(const typename
           if (o0 + j <= oe && z >= 0 && z < R.nin) y[j] = cadd(y[j], cmul(sv[z * nt + tid], kl));
         }
       }
+    }
     }
 #pragma unroll
     for (int j = 0; j < kOutChunk; j += 2) {
