@@ -528,6 +528,7 @@ typedef struct {
   int group;              /* consecutive planes summed into one transform plane (scan_avg); >= 1 */
   const void* mask0;      /* optional nx*ny row-major multipliers of every plane (NULL: none) */
   const void* mask1;
+  const void* data2;      /* optional second volume of the same layout, added element-wise (NULL: none) */
 } mm_scan_planes;
 
 typedef struct {

@@ -68,7 +68,7 @@ class LocalDesc(Structure):
 class ScanPlanes(Structure):
     _fields_ = [("data", c_void_p), ("s0", ctypes.c_longlong), ("s1", ctypes.c_longlong), ("s2", ctypes.c_longlong),
                 ("nx", c_int), ("ny", c_int), ("nz", c_int), ("group", c_int), ("mask0", c_void_p),
-                ("mask1", c_void_p)]
+                ("mask1", c_void_p), ("data2", c_void_p)]
 
 
 class ScanDesc(Structure):

@@ -40,12 +40,17 @@ def real_dtype(t):
     raise ValueError(f"plane convolution supports float32 and float64 data, got {t.dtype}")
 
 
-def planes_record(t, *, group=1, masks=(None, None)):
-    """ScanPlanes of a 3-D device tensor (any strides), optional XY masks."""
+def planes_record(t, *, group=1, masks=(None, None), add=None):
+    """ScanPlanes of a 3-D device tensor (any strides), optional XY masks and
+    an optional second tensor of the same shape and strides added to it."""
     s = t.stride()
     m0, m1 = masks
+    if add is not None and (tuple(add.shape) != tuple(t.shape) or add.stride() != t.stride()
+                            or add.dtype != t.dtype):
+        raise ValueError("the added volume must share the source's shape, strides and type")
     return _lib.ScanPlanes(t.data_ptr(), s[0], s[1], s[2], t.shape[0], t.shape[1], t.shape[2], int(group),
-                           None if m0 is None else m0.data_ptr(), None if m1 is None else m1.data_ptr())
+                           None if m0 is None else m0.data_ptr(), None if m1 is None else m1.data_ptr(),
+                           None if add is None else add.data_ptr())
 
 
 class KernelSpectrum:
@@ -77,7 +82,8 @@ class KernelSpectrum:
         self._keep = kernel  # the kernel stays alive until the stream has read it
 
     def convolve(self, src, *, zrule, out, crop, out_shape, out_planes, zoff=0, group=1, masks=(None, None),
-                 wrap=None, accumulate=False, alpha=1.0, src_spectra=None, out_spectra=None, out_weight=None):
+                 wrap=None, accumulate=False, alpha=1.0, src_spectra=None, out_spectra=None, out_weight=None,
+                 add=None):
         """One engine pass of ``src`` (3-D device tensor) into ``out``.
 
         ``src_spectra``: the source's packed spectra (``forward_spectra``),
@@ -88,7 +94,7 @@ class KernelSpectrum:
         lib = _lib.load()
         if src.dtype != self.dtype or (out is not None and out.dtype != self.dtype):
             raise ValueError("source, kernel and output must share one floating type")
-        rec = planes_record(src, group=group, masks=masks)
+        rec = planes_record(src, group=group, masks=masks, add=add)
         nin = -(-int(src.shape[2]) // int(group))
         conv = conv_record(src, rec, wrap, zrule, zoff, out_planes, crop, out_shape, out, accumulate, alpha)
         conv.src_spectra = None if src_spectra is None else src_spectra.data_ptr()

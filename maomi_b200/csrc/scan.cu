@@ -98,6 +98,7 @@ struct Planes {
   int nx, ny, nz, group, planes;  // planes = ceil(nz / group)
   const void* m0;
   const void* m1;
+  const void* data2;  // optional second volume (same strides), added element-wise
   int wrap, wx0, wy0, ext_x, ext_y;
 };
 
@@ -115,7 +116,12 @@ __device__ __forceinline__ T plane_value(const Planes& P, int i, int j, int p) {
   const int z0 = p * P.group;
   const int z1 = min(z0 + P.group, P.nz);
   T s = T(0);
-  for (int z = z0; z < z1; ++z) s += d[base + (long long)z * P.s2];
+  if (P.data2) {
+    const T* d2 = static_cast<const T*>(P.data2);
+    for (int z = z0; z < z1; ++z) s += d[base + (long long)z * P.s2] + d2[base + (long long)z * P.s2];
+  } else {
+    for (int z = z0; z < z1; ++z) s += d[base + (long long)z * P.s2];
+  }
   if (P.m0) s *= static_cast<const T*>(P.m0)[(long long)x * P.ny + y];
   if (P.m1) s *= static_cast<const T*>(P.m1)[(long long)x * P.ny + y];
   return s;
@@ -469,7 +475,7 @@ struct BgVols {
 
 template <class T>
 __global__ void background_kernel(BgVols<T> V, int nvol, long long s0, long long s1, long long s2, int nx, int ny,
-                                  const int32_t* __restrict__ idx, const double* __restrict__ scale, int n,
+                                  int nz, const int32_t* __restrict__ idx, const double* __restrict__ scale, int n,
                                   double power, const T* __restrict__ mask, T* __restrict__ out) {
   const long long np = (long long)nx * ny;
   for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < np; e += (long long)gridDim.x * blockDim.x) {
@@ -478,7 +484,10 @@ __global__ void background_kernel(BgVols<T> V, int nvol, long long s0, long long
     double acc = 0.0;
     for (int v = 0; v < nvol; ++v) {
       double s = 0.0;
-      for (int i = 0; i < n; ++i) s += double(V.v[v][base + (long long)idx[i] * s2]) * scale[i];
+      for (int i = 0; i < n; ++i) {
+        const int z = idx[i];
+        if (z >= 0 && z < nz) s += double(V.v[v][base + (long long)z * s2]) * scale[i];  // host-checked; never read out of range
+      }
       acc += s / n;
     }
     acc *= power;
@@ -589,6 +598,7 @@ Planes make_planes(const mm_scan_planes* p, int wrap, int wx0, int wy0, int ext_
   P.planes = (p->nz + p->group - 1) / p->group;
   P.m0 = p->mask0;
   P.m1 = p->mask1;
+  P.data2 = p->data2;
   P.wrap = wrap;
   P.wx0 = wx0;
   P.wy0 = wy0;
@@ -793,13 +803,13 @@ extern "C" int mm_scan_background(int fp64, const void* const* volumes, int nvol
   if (fp64) {
     scan::BgVols<double> V{};
     for (int v = 0; v < nvol; ++v) V.v[v] = static_cast<const double*>(volumes[v]);
-    scan::background_kernel<double><<<blocks, 256, 0, st>>>(V, nvol, s0, s1, s2, nx, ny, idx, scale, n, power,
+    scan::background_kernel<double><<<blocks, 256, 0, st>>>(V, nvol, s0, s1, s2, nx, ny, nz, idx, scale, n, power,
                                                             static_cast<const double*>(mask),
                                                             static_cast<double*>(out));
   } else {
     scan::BgVols<float> V{};
     for (int v = 0; v < nvol; ++v) V.v[v] = static_cast<const float*>(volumes[v]);
-    scan::background_kernel<float><<<blocks, 256, 0, st>>>(V, nvol, s0, s1, s2, nx, ny, idx, scale, n, power,
+    scan::background_kernel<float><<<blocks, 256, 0, st>>>(V, nvol, s0, s1, s2, nx, ny, nz, idx, scale, n, power,
                                                            static_cast<const float*>(mask), static_cast<float*>(out));
   }
   MM_CHECK_LAUNCH("scan background");

@@ -210,3 +210,92 @@ def blurred_background(volume, indices, kernel, *, power_ratio=1.0, mask=None, z
     spec.convolve(image[..., None], zrule=_lib.MM_SCAN_EACH_Z, out=out, crop=(a // 2, b // 2), out_shape=(X, Y),
                   out_planes=1)
     return _result(out, volume)
+
+
+class FrameScanner:
+    """The optical part of one frame of the reference's planar movie loop
+    (maomi/movie.py:601-679), on the device: the focal slab of the frame's
+    activity volume plus the static base, convolved with the PSF over
+    ``scan_avg`` plane groups (``single_scan``); the optional extra blur
+    (``conv2_same`` of the frame onto itself); and both out-of-focus tails as
+    blurred backgrounds of the planes above and below the slab
+    (``blurred_background`` with the frequency-domain kernels).  The spectra
+    of the PSF, the tail kernels and the blur are built once for the volume
+    shape; each frame is then one engine pass for the slab (the base is added
+    in the read) and one per tail.  Motion, binning and detector noise follow
+    in the reference loop and are not part of this class.
+
+    ``tails``: up to two dicts (top, bottom) with ``kernel`` (2-D, already
+    normalised to unit sum), ``weight``, ``mask`` (2-D) and ``zscale``.
+    """
+
+    def __init__(self, shape, psf, *, scan_avg=2, tails=(), blur=None, device=None):
+        import torch
+        dev = device if device is not None else _device_of(psf)
+        _lib.require_cuda(dev)
+        p = as_device(psf, dev, torch.float32)
+        if p.ndim != 3 or len(shape) != 3:
+            raise ValueError("FrameScanner needs an X,Y,Z volume shape and an X,Y,Z PSF")
+        self.shape, self.depth, self.device = tuple(int(s) for s in shape), int(p.shape[2]), dev
+        self.scan_avg = _check_group(scan_avg)
+        self.psf_xy = (int(p.shape[0]), int(p.shape[1]))
+        self.freq = FrequencyPSF(self.shape, p, self.scan_avg, dev)
+        if len(tails) not in (0, 2):
+            raise ValueError("Both optical tails are required")
+        X, Y = self.shape[:2]
+        self.tails = []
+        for spec in tails:
+            mask = None if spec.get("mask") is None else mask_tensor(spec["mask"], (X, Y), dev, torch.float32)
+            zs = spec.get("zscale")
+            self.tails.append({"kernel": FrequencyPSF(self.shape, as_device(spec["kernel"], dev, torch.float32), 1,
+                                                      dev),
+                               "weight": float(spec["weight"]), "mask": mask,
+                               "zscale": None if zs is None else np.asarray(zs, np.float64).ravel()})
+        self.blur = None
+        if blur is not None:
+            k = as_device(blur, dev, torch.float32)
+            a, b = int(k.shape[0]), int(k.shape[1])
+            self.blur = (KernelSpectrum(k[..., None].contiguous(), transform_size(X + max(a // 2, a - 1 - a // 2)),
+                                        transform_size(Y + max(b // 2, b - 1 - b // 2))), (a // 2, b // 2))
+
+    def frame(self, temp, base, z, *, scale=1.0, sf=2.0):
+        """The optical frame (X, Y) device tensor for focal slab planes
+        [z, z + depth): movie.py:650-679 before the row motion."""
+        import torch
+        t = as_device(temp, self.device, torch.float32).contiguous()
+        b = as_device(base, self.device, torch.float32).contiguous()
+        X, Y, nz = self.shape
+        if tuple(t.shape) != self.shape or tuple(b.shape) != self.shape:
+            raise ValueError(f"frame volumes must have shape {self.shape}")
+        z = int(z)
+        if z < 0 or z + self.depth > nz:
+            raise ValueError("Motion places focal slab outside volume")
+        out = torch.empty((X, Y), dtype=torch.float32, device=self.device)
+        a, bb = self.psf_xy
+        self.freq.kernel.convolve(t[:, :, z:z + self.depth], zrule=_lib.MM_SCAN_SUM_Z, out=out, crop=(a // 2, bb // 2),
+                                  out_shape=(X, Y), out_planes=1, group=self.scan_avg, alpha=scale / (2 * sf * sf),
+                                  add=b[:, :, z:z + self.depth])
+        if self.blur is not None:
+            spec, crop = self.blur
+            spec.convolve(out[..., None], zrule=_lib.MM_SCAN_EACH_Z, out=out, crop=crop, out_shape=(X, Y),
+                          out_planes=1, accumulate=True)
+        for j, spec in enumerate(self.tails):
+            idx = np.arange(z) if j == 0 else np.arange(z + self.depth, nz)
+            zs = spec["zscale"]
+            if len(idx) == 0:
+                idx, zs = np.arange(nz), None
+            scl = zs[:len(idx)] if zs is not None and zs.size >= len(idx) else np.ones(len(idx))
+            image = torch.empty((X, Y), dtype=torch.float32, device=self.device)
+            ptrs = (_lib.c_void_p * 2)(t.data_ptr(), b.data_ptr())
+            s = t.stride()
+            # both tables stay referenced until the launch is queued: a table
+            # freed early would hand its block to the next upload, whose copy
+            # (queued before the launch) would overwrite it
+            idx_d = _lib.upload(idx.astype(np.int32), self.device)
+            scl_d = _lib.upload(scl.astype(np.float64), self.device)
+            _lib.call("mm_scan_background", 0, ptrs, 2, s[0], s[1], s[2], X, Y, nz, _lib.ptr(idx_d), _lib.ptr(scl_d),
+                      len(idx), spec["weight"], _lib.ptr(spec["mask"]), _lib.ptr(image), _lib.stream_of(self.device))
+            k = spec["kernel"]
+            k.kernel.convolve(image[..., None], zrule=_lib.MM_SCAN_EACH_Z, out=out, crop=k.background_crop,
+                              out_shape=(X, Y), out_planes=1, accumulate=True, alpha=scale / (sf * sf))
+        return out
