@@ -480,6 +480,10 @@ int mm_surrogate_layout(long long* offsets, int n);
 int mm_surrogate_constants(void* F, void* G, void* FT, void* GT, void* stream);
 /* Prediction y for d->sites sites (refreshes the BF16 weight copies first). */
 int mm_surrogate_forward(const mm_surrogate_desc* d, int check, void* stream);
+/* Inference: the forward pass with the projection writing the PSF planes
+ * planes (S,9,64,64) FP32, negatives clipped to 0, instead of y (the
+ * equivalent of mm_surrogate_forward followed by mm_surrogate_planes). */
+int mm_surrogate_predict(const mm_surrogate_desc* d, float* planes, int check, void* stream);
 /* Loss (mean over sites of ||y - t||^2 / ||t||^2, planes 0..8) and every
  * parameter gradient into d->grads, after mm_surrogate_forward on the same d.
  * target: (S,4096,16) FP32. */

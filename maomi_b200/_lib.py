@@ -115,6 +115,7 @@ SIGNATURES = {
     "mm_surrogate_inputs": (c_int, [c_void_p, c_void_p, c_int, c_int, c_void_p, c_float, c_void_p, c_void_p, c_int,
                                     c_void_p, c_void_p, c_void_p, c_int, c_void_p]),
     "mm_surrogate_planes": (c_int, [c_void_p, c_void_p, c_int, c_void_p]),
+    "mm_surrogate_predict": (c_int, [POINTER(SurrogateDesc), c_void_p, c_int, c_void_p]),
     "mm_gather_screens": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int, c_int, c_int, c_int, c_void_p]),
     "mm_resample_power": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int,
                                   c_int, c_int, c_int, c_int, c_int, c_int, c_int, c_float, c_void_p]),

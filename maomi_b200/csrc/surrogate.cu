@@ -15,22 +15,31 @@ namespace mm {
 namespace {
 
 // ------------------------------------------------------------ launching --
-template <int NT, int NB, class Epi, int ST = gemm::kStages>
+// One persistent CTA per SM over the grid.x * grid.y tiles of `t`.
+template <int NT, int NB, class Epi>
 int launch_gemm(const CUtensorMap& a, const CUtensorMap& b, const CUtensorMap& a2, const CUtensorMap& b2,
-                const gemm::Tiles& t, dim3 grid, const Epi& epi, cudaStream_t s) {
-  auto kernel = gemm::gemm_kernel<NT, NB, Epi, ST>;
-  const size_t smem = gemm::Smem<NT, NB, ST>::bytes;
+                gemm::Tiles t, dim3 grid, const Epi& epi, cudaStream_t s) {
+  auto kernel = gemm::gemm_kernel<NT, NB, Epi>;
+  const size_t smem = gemm::Smem<NT, NB>::bytes;
   MM_CHECK_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
                 "cudaFuncSetAttribute(gemm)");
-  int per_sm = 0;
-  MM_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 128, smem), "occupancy(gemm)");
-  constexpr int cols = (int)gemm::tmem_cols<(NT > 8 * NB ? NT : 8 * NB)>();
+  int per_sm = 0, device = 0, sms = 0;
+  MM_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, gemm::kThreads, smem),
+                "occupancy(gemm)");
+  constexpr int cols = 2 * (int)gemm::tmem_cols<(NT > 8 * NB ? NT : 8 * NB)>();
   if (per_sm < 1 || per_sm * cols > 512) {
     set_error("GEMM tile %dx%d: %d CTAs per SM would not fit tensor memory", 128, NT, per_sm);
     return MM_ERR_UNSUPPORTED;
   }
   if (grid.x == 0 || grid.y == 0) return MM_OK;
-  kernel<<<grid, 128, smem, s>>>(a, b, a2, b2, t, epi);
+  MM_CHECK_CUDA(cudaGetDevice(&device), "cudaGetDevice");
+  MM_CHECK_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "SM count");
+  const long long ntiles = (long long)grid.x * grid.y;
+  MM_CHECK_ARG(ntiles < (1ll << 31), "GEMM: %lld tiles exceed the tile index range", ntiles);
+  t.grid_x = (int)grid.x;
+  t.ntiles = (int)ntiles;
+  const int ctas = (int)std::min<long long>(ntiles, (long long)sms * per_sm);
+  kernel<<<ctas, gemm::kThreads, smem, s>>>(a, b, a2, b2, t, epi);
   MM_CHECK_LAUNCH("tcgen05 GEMM");
   return MM_OK;
 }
@@ -40,7 +49,7 @@ struct StoreF32 {
   float* d;
   int m, n, nt;
   long long ld;
-  __device__ void store(int bx, int by, int row, int c, const float (&v)[32]) const {
+  __device__ void store(int bx, int by, int row, int c, const float (&v)[32], unsigned char* scratch) const {
     const int r = bx * gemm::kBM + row;
     if (r >= m) return;
     const int c0 = by * nt + c;
@@ -73,13 +82,21 @@ int gemm_tn(const void* a, const void* b, float* d, int m, int n, int k, int* er
 constexpr int kGrid = 64, kPix = 4096, kWidth = 32, kModes = 12, kNModes = 288, kRows = 576;
 constexpr int kPlanes = 9, kOut = 16, kLayers = 4, kCin = 18, kGroup = 8;  // sites per wide tile
 
+// tanh-form GELU on the hardware tanh approximation (PTX tanh.approx.f32,
+// relative error about 2^-11, below the BF16 rounding of the layer outputs).
+__device__ __forceinline__ float tanh_hw(float x) {
+  float y;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
 __device__ __forceinline__ float gelu(float z) {
-  const float u = 0.7978845608028654f * (z + 0.044715f * z * z * z);
-  return 0.5f * z * (1.f + tanhf(u));
+  const float u = 0.7978845608028654f * fmaf(0.044715f * z, z * z, z);
+  const float hz = 0.5f * z;
+  return fmaf(hz, tanh_hw(u), hz);
 }
 __device__ __forceinline__ float gelu_grad(float z) {
-  const float u = 0.7978845608028654f * (z + 0.044715f * z * z * z);
-  const float t = tanhf(u);
+  const float u = 0.7978845608028654f * fmaf(0.044715f * z, z * z, z);
+  const float t = tanh_hw(u);
   return 0.5f * (1.f + t) + 0.5f * z * (1.f - t * t) * 0.7978845608028654f * (1.f + 3.f * 0.044715f * z * z);
 }
 
@@ -118,7 +135,7 @@ __global__ void spectral_constants_kernel(__nv_bfloat16* F, __nv_bfloat16* G, __
 struct EpiSpectral {
   float* out;  // (S, 576, 32)
   int sites;
-  __device__ void store(int bx, int by, int row, int c, const float (&v)[32]) const {
+  __device__ void store(int bx, int by, int row, int c, const float (&v)[32], unsigned char* scratch) const {
     const int r = bx * gemm::kBM + row, s = by * kGroup + c / kWidth;
     if (r >= kRows || s >= sites) return;
     float4* dst = reinterpret_cast<float4*>(out + ((size_t)s * kRows + r) * kWidth);
@@ -147,18 +164,65 @@ __device__ __forceinline__ void store_both(__nv_bfloat16* hp, __nv_bfloat16* hc,
   for (int o = 0; o < kWidth; ++o) dc[(size_t)o * kPix] = __float2bfloat16_rn(h[o]);
 }
 
+// The same two stores from a whole warp whose lanes hold 32 consecutive
+// pixels of site s (lane l: pixel pix0 + l).  The pixel-major rows go out
+// through the warp's 1 KB shared scratch, 16 rows at a time, as 512-byte
+// contiguous runs (four full-line requests per store instruction instead of
+// sixteen half-filled ones); 16-byte pieces are XOR-swizzled by row pair so
+// both the row writes and the linear reads are free of bank conflicts.
+__device__ __forceinline__ void store_both_warp(__nv_bfloat16* hp, __nv_bfloat16* hc, int s, int pix,
+                                                const float (&h)[32], unsigned char* scratch) {
+  const int lane = threadIdx.x & 31, pix0 = pix - lane;
+  uint4 u[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    __nv_bfloat162 a = __floats2bfloat162_rn(h[8 * k], h[8 * k + 1]), b = __floats2bfloat162_rn(h[8 * k + 2], h[8 * k + 3]);
+    __nv_bfloat162 c = __floats2bfloat162_rn(h[8 * k + 4], h[8 * k + 5]), d = __floats2bfloat162_rn(h[8 * k + 6], h[8 * k + 7]);
+    u[k].x = *reinterpret_cast<uint32_t*>(&a);
+    u[k].y = *reinterpret_cast<uint32_t*>(&b);
+    u[k].z = *reinterpret_cast<uint32_t*>(&c);
+    u[k].w = *reinterpret_cast<uint32_t*>(&d);
+  }
+#pragma unroll
+  for (int half = 0; half < 2; ++half) {
+    if ((lane >> 4) == half) {
+      const int r = lane & 15, g = (r >> 1) & 3;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) *reinterpret_cast<uint4*>(scratch + r * 64 + ((k ^ g) << 4)) = u[k];
+    }
+    __syncwarp();
+    uint4* dst = reinterpret_cast<uint4*>(hp + ((size_t)s * kPix + pix0 + 16 * half) * kWidth);
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      const int m = lane + 32 * i, r = m >> 2, g = (r >> 1) & 3;
+      dst[m] = *reinterpret_cast<const uint4*>(scratch + r * 64 + (((m & 3) ^ g) << 4));
+    }
+    __syncwarp();
+  }
+  if (!hc) return;
+  __nv_bfloat16* dc = hc + (size_t)s * kWidth * kPix + pix;
+#pragma unroll
+  for (int o = 0; o < kWidth; ++o) dc[(size_t)o * kPix] = __float2bfloat16_rn(h[o]);
+}
+
 // Layer output: z = acc + bias; h = gelu(z) (or z); z kept (FP32) for the backward pass.
 struct EpiLayer {
   const float* bias;
   float* z;  // (S, 4096, 32) or NULL
   __nv_bfloat16 *hp, *hc;  // hc NULL: pixel-major copy only
   int sites, act;
-  __device__ void store(int bx, int by, int row, int c, const float (&v)[32]) const {
+  __device__ void store(int bx, int by, int row, int c, const float (&v)[32], unsigned char* scratch) const {
     const int pix = bx * gemm::kBM + row, s = by * kGroup + c / kWidth;
     if (s >= sites) return;
     float h[32];
 #pragma unroll
-    for (int o = 0; o < 32; ++o) h[o] = v[o] + __ldg(bias + o);
+    for (int k = 0; k < 8; ++k) {
+      const float4 b = __ldg(reinterpret_cast<const float4*>(bias) + k);
+      h[4 * k] = v[4 * k] + b.x;
+      h[4 * k + 1] = v[4 * k + 1] + b.y;
+      h[4 * k + 2] = v[4 * k + 2] + b.z;
+      h[4 * k + 3] = v[4 * k + 3] + b.w;
+    }
     if (z) {
       float4* dz = reinterpret_cast<float4*>(z + ((size_t)s * kPix + pix) * kWidth);
 #pragma unroll
@@ -168,7 +232,7 @@ struct EpiLayer {
 #pragma unroll
       for (int o = 0; o < 32; ++o) h[o] = gelu(h[o]);
     }
-    store_both(hp, hc, s, pix, h);
+    store_both_warp(hp, hc, s, pix, h, scratch);
   }
 };
 
@@ -177,7 +241,7 @@ struct EpiBack {
   const float* zprev;  // (S, 4096, 32) or NULL (no activation)
   __nv_bfloat16 *dp, *dc;
   int sites;
-  __device__ void store(int bx, int by, int row, int c, const float (&v)[32]) const {
+  __device__ void store(int bx, int by, int row, int c, const float (&v)[32], unsigned char* scratch) const {
     const int pix = bx * gemm::kBM + row, s = by * kGroup + c / kWidth;
     if (s >= sites) return;
     float d[32];
@@ -195,7 +259,7 @@ struct EpiBack {
 #pragma unroll
       for (int o = 0; o < 32; ++o) d[o] = v[o];
     }
-    store_both(dp, dc, s, pix, d);
+    store_both_warp(dp, dc, s, pix, d, scratch);
   }
 };
 
@@ -205,7 +269,7 @@ struct EpiProject {
   const float* base;  // (4096, 16)
   float* y;           // (S, 4096, 16)
   int sites;
-  __device__ void store(int bx, int by, int row, int c, const float (&v)[32]) const {
+  __device__ void store(int bx, int by, int row, int c, const float (&v)[32], unsigned char* scratch) const {
     const int pix = bx * gemm::kBM + row;
 #pragma unroll
     for (int half = 0; half < 2; ++half) {
@@ -224,13 +288,44 @@ struct EpiProject {
   }
 };
 
+// Inference projection straight to the PSF planes: out (S, 9, 4096) =
+// max(acc + bias + base, 0) for the first 9 output channels, one coalesced
+// word per plane and pixel (the 16-channel y is not written).
+struct EpiPlanes {
+  const float* bias;  // (16)
+  const float* base;  // (4096, 16)
+  float* out;         // (S, 9, 4096)
+  int sites;
+  __device__ void store(int bx, int by, int row, int c, const float (&v)[32], unsigned char* scratch) const {
+    const int pix = bx * gemm::kBM + row;
+    const float4* b4 = reinterpret_cast<const float4*>(base + (size_t)pix * kOut);
+    float b[12];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const float4 u = __ldg(b4 + k);
+      b[4 * k] = u.x + __ldg(bias + 4 * k);
+      b[4 * k + 1] = u.y + __ldg(bias + 4 * k + 1);
+      b[4 * k + 2] = u.z + __ldg(bias + 4 * k + 2);
+      b[4 * k + 3] = u.w + __ldg(bias + 4 * k + 3);
+    }
+#pragma unroll
+    for (int half = 0; half < 2; ++half) {
+      const int s = by * kGroup + c / kOut + half;
+      if (s >= sites) continue;
+      float* dst = out + (size_t)s * kPlanes * kPix + pix;
+#pragma unroll
+      for (int k = 0; k < kPlanes; ++k) dst[(size_t)k * kPix] = fmaxf(v[16 * half + k] + b[k], 0.f);
+    }
+  }
+};
+
 // Weight gradient: the tile's rows are (site, a) pairs (rb rows per site), its
 // columns (site', b) pairs (32 per site); only site == site' blocks belong to
 // the gradient dW[a][b] (FP32, accumulated over all tiles).
 struct EpiWeightGrad {
   float* dw;  // (rb, 32)
   int rb, sites;
-  __device__ void store(int bx, int by, int row, int c, const float (&v)[32]) const {
+  __device__ void store(int bx, int by, int row, int c, const float (&v)[32], unsigned char* scratch) const {
     const int per_tile = gemm::kBM / rb;
     const int j = row / rb, a = row % rb;
     if (c / kWidth != j || bx * per_tile + j >= sites) return;
@@ -241,34 +336,98 @@ struct EpiWeightGrad {
 
 // ------------------------------------------------------- spectral mixing
 // Vo_q = V_q R_q (complex, per mode): V (S, 576, 32) FP32 -> Voc (S*32, 576) BF16.
+//
+// A block owns 8 consecutive modes q0..q0+7 and walks the groups of
+// kMixStage sites g = blockIdx.y, blockIdx.y + gridDim.y, ... (one resident
+// wave of blocks).  Thread (m, o) = (lane % 8, 4 * warp + lane / 8) keeps
+// column o of R_{q0+m} (32 complex weights) in registers, so the inner loop
+// reads only the staged V rows (float4 loads, conflict-free with a 36-float
+// row pitch); the next group's rows are loaded into registers while the
+// current group is mixed, and every store of a warp covers four whole
+// 32-byte segments of Voc (8 modes x re/im of one (site, channel) row).
+constexpr int kMixModes = 8, kMixStage = 8, kMixPitch = 36;
+
 __global__ void __launch_bounds__(256) mix_forward_kernel(const float* __restrict__ V, const float* __restrict__ Rr,
                                                           const float* __restrict__ Ri, __nv_bfloat16* __restrict__ Voc,
                                                           int sites) {
-  __shared__ float rr[32][33], ri[32][33], vr[8][32], vi[8][32];
-  const int q = blockIdx.x, t = threadIdx.x;
-  for (int e = t; e < 1024; e += 256) {
-    rr[e / 32][e % 32] = Rr[(size_t)q * 1024 + e];
-    ri[e / 32][e % 32] = Ri[(size_t)q * 1024 + e];
+  __shared__ __align__(16) float vr[kMixStage][kMixModes][kMixPitch];
+  __shared__ __align__(16) float vi[kMixStage][kMixModes][kMixPitch];
+  const int t = threadIdx.x, lane = t & 31, m = lane & 7, o = 4 * (t >> 5) + (lane >> 3);
+  const int q0 = blockIdx.x * kMixModes, q = q0 + m;
+  const int groups = (sites + kMixStage - 1) / kMixStage;
+  // staged float4 f = t + 256 k of a group: site f / 128, row (f / 8) % 16, column quad f % 8
+  auto load_group = [&](int gi, float4 (&r)[4]) {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int f = t + 256 * k, s = gi * kMixStage + (f >> 7), row = (f >> 3) & 15, c4 = f & 7;
+      r[k] = s < sites ? __ldg(reinterpret_cast<const float4*>(V + ((size_t)s * kRows + 2 * q0 + row) * kWidth) + c4)
+                       : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+  };
+  float4 pre[4];
+  if (blockIdx.y < groups) load_group(blockIdx.y, pre);
+  float wr[32], wi[32];
+#pragma unroll
+  for (int i = 0; i < 32; ++i) {
+    wr[i] = __ldg(Rr + (size_t)q * 1024 + i * 32 + o);
+    wi[i] = __ldg(Ri + (size_t)q * 1024 + i * 32 + o);
   }
-  const int sl = t / 32, o = t % 32;
-  for (int s0 = blockIdx.y * 64; s0 < min(sites, blockIdx.y * 64 + 64); s0 += 8) {
+  for (int gi = blockIdx.y; gi < groups; gi += gridDim.y) {
+    __syncthreads();  // the previous group's rows have been read
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int f = t + 256 * k, sl = f >> 7, row = (f >> 3) & 15, c4 = f & 7;
+      float* dst = (row & 1) ? &vi[sl][row >> 1][4 * c4] : &vr[sl][row >> 1][4 * c4];
+      *reinterpret_cast<float4*>(dst) = pre[k];
+    }
     __syncthreads();
-    {
+    if (gi + (int)gridDim.y < groups) load_group(gi + gridDim.y, pre);  // in flight during the mixing below
+    const int s0 = gi * kMixStage;
+    // two sites at a time (four independent FMA chains); rows of sites past
+    // the end were staged as zeros and their results are not stored
+#pragma unroll 1
+    for (int sl = 0; sl < kMixStage; sl += 2) {
+      float re0 = 0.f, im0 = 0.f, re1 = 0.f, im1 = 0.f;
+#pragma unroll
+      for (int i4 = 0; i4 < 8; ++i4) {
+        const float4 a0 = *reinterpret_cast<const float4*>(&vr[sl][m][4 * i4]);
+        const float4 b0 = *reinterpret_cast<const float4*>(&vi[sl][m][4 * i4]);
+        const float4 a1 = *reinterpret_cast<const float4*>(&vr[sl + 1][m][4 * i4]);
+        const float4 b1 = *reinterpret_cast<const float4*>(&vi[sl + 1][m][4 * i4]);
+        const float x0[4] = {a0.x, a0.y, a0.z, a0.w}, y0[4] = {b0.x, b0.y, b0.z, b0.w};
+        const float x1[4] = {a1.x, a1.y, a1.z, a1.w}, y1[4] = {b1.x, b1.y, b1.z, b1.w};
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const int i = 4 * i4 + j;
+          re0 = fmaf(x0[j], wr[i], fmaf(-y0[j], wi[i], re0));
+          im0 = fmaf(x0[j], wi[i], fmaf(y0[j], wr[i], im0));
+          re1 = fmaf(x1[j], wr[i], fmaf(-y1[j], wi[i], re1));
+          im1 = fmaf(x1[j], wi[i], fmaf(y1[j], wr[i], im1));
+        }
+      }
       const int s = s0 + sl;
-      vr[sl][o] = s < sites ? V[((size_t)s * kRows + 2 * q) * kWidth + o] : 0.f;
-      vi[sl][o] = s < sites ? V[((size_t)s * kRows + 2 * q + 1) * kWidth + o] : 0.f;
+      if (s < sites)
+        *reinterpret_cast<__nv_bfloat162*>(Voc + ((size_t)s * kWidth + o) * kRows + 2 * q) =
+            __floats2bfloat162_rn(re0, im0);
+      if (s + 1 < sites)
+        *reinterpret_cast<__nv_bfloat162*>(Voc + ((size_t)(s + 1) * kWidth + o) * kRows + 2 * q) =
+            __floats2bfloat162_rn(re1, im1);
     }
-    __syncthreads();
-    float re = 0.f, im = 0.f;
-#pragma unroll 8
-    for (int i = 0; i < 32; ++i) {
-      re += vr[sl][i] * rr[i][o] - vi[sl][i] * ri[i][o];
-      im += vr[sl][i] * ri[i][o] + vi[sl][i] * rr[i][o];
-    }
-    const int s = s0 + sl;
-    if (s < sites)
-      *reinterpret_cast<__nv_bfloat162*>(Voc + ((size_t)s * kWidth + o) * kRows + 2 * q) = __floats2bfloat162_rn(re, im);
   }
+}
+
+// One resident wave of mixing blocks: 36 mode groups x as many site-group
+// walkers as fit beside them.
+int mix_forward(const float* V, const float* Rr, const float* Ri, __nv_bfloat16* Voc, int S, cudaStream_t s) {
+  int device = 0, sms = 0, per_sm = 0;
+  MM_CHECK_CUDA(cudaGetDevice(&device), "cudaGetDevice");
+  MM_CHECK_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "SM count");
+  MM_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, mix_forward_kernel, 256, 0), "occupancy(mix)");
+  const int groups = (S + kMixStage - 1) / kMixStage;
+  const int walkers = std::max(1, std::min(groups, sms * std::max(per_sm, 1) / (kNModes / kMixModes)));
+  mix_forward_kernel<<<dim3(kNModes / kMixModes, walkers), 256, 0, s>>>(V, Rr, Ri, Voc, S);
+  MM_CHECK_LAUNCH("surrogate spectral mixing");
+  return MM_OK;
 }
 
 // Backward of the mixing for one mode over all sites: dV (-> dVc BF16) and dR.
@@ -497,11 +656,24 @@ __global__ void gather_inputs_kernel(const float* __restrict__ pooled, int Hp, i
 }
 
 // Prediction (S, 4096, 16) -> PSF planes (S, 9, 64, 64), negative values clipped.
-__global__ void psf_planes_kernel(const float* __restrict__ y, float* __restrict__ out, int sites) {
-  const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (idx >= (long long)sites * kPlanes * kPix) return;
-  const int s = int(idx / (kPlanes * kPix)), r = int(idx % (kPlanes * kPix)), k = r / kPix, p = r % kPix;
-  out[idx] = fmaxf(y[((size_t)s * kPix + p) * kOut + k], 0.f);
+// y (S, 4096, 16) -> planes (S, 9, 4096), negatives clipped: one thread per
+// pixel reads its 64-byte output row and writes one coalesced word per plane.
+constexpr int kPlanePixels = 128;
+__global__ void __launch_bounds__(kPlanePixels) psf_planes_kernel(const float* __restrict__ y, float* __restrict__ out) {
+  const int s = blockIdx.y, pix = blockIdx.x * kPlanePixels + threadIdx.x;
+  const float4* src = reinterpret_cast<const float4*>(y + ((size_t)s * kPix + pix) * kOut);
+  float v[12];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const float4 a = __ldg(src + k);
+    v[4 * k] = a.x;
+    v[4 * k + 1] = a.y;
+    v[4 * k + 2] = a.z;
+    v[4 * k + 3] = a.w;
+  }
+  float* dst = out + (size_t)s * kPlanes * kPix + pix;
+#pragma unroll
+  for (int k = 0; k < kPlanes; ++k) dst[(size_t)k * kPix] = fmaxf(v[k], 0.f);
 }
 
 
@@ -558,9 +730,7 @@ int fused(const void* A, const void* coef_c, const void* act_p, const void* W, i
   t.ncols = 256;
   t.err = err;
   const dim3 grid(kPix / gemm::kBM, (S + kGroup - 1) / kGroup);
-  // short K (9 blocks + 8 pointwise blocks) and a heavy epilogue: a 2-stage
-  // ring fits two CTAs per SM, so one CTA's epilogue overlaps the other's loads
-  return launch_gemm<256, 32, Epi, 2>(m.a, m.b, m.a2, m.b2, t, grid, epi, s);
+  return launch_gemm<256, 32>(m.a, m.b, m.a2, m.b2, t, grid, epi, s);
 }
 
 // Pointwise-only GEMM: acc[pix, (site, n)] = act_p (S*4096 x kin) * W (NB x kin)^T per site.
@@ -576,7 +746,7 @@ int pointwise(const void* act_p, int kin, const void* W, int S, int* err, const 
   t.ncols = kGroup * NB;
   t.err = err;
   const dim3 grid(kPix / gemm::kBM, (S + kGroup - 1) / kGroup);
-  return launch_gemm<kGroup * NB, NB, Epi, 2>(m.a2, m.b2, m.a2, m.b2, t, grid, epi, s);
+  return launch_gemm<kGroup * NB, NB>(m.a2, m.b2, m.a2, m.b2, t, grid, epi, s);
 }
 
 // Weight gradient dW[a][b] += sum_(site,pix) g[(site, a), pix] * act[(site, b), pix]
@@ -704,10 +874,11 @@ extern "C" int mm_surrogate_constants(void* F, void* G, void* FT, void* GT, void
   return MM_OK;
 }
 
-extern "C" int mm_surrogate_forward(const mm_surrogate_desc* d, int check, void* stream) {
-  using namespace mm;
-  if (int rc = check_desc(d, false)) return rc;
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
+namespace mm {
+namespace {
+// The forward pass; with `planes` the projection writes the clipped PSF
+// planes (S, 9, 4096) instead of the prediction d->y.
+int forward_pass(const mm_surrogate_desc* d, float* planes, cudaStream_t s) {
   const int S = d->sites;
   if (int rc = refresh_weights(d, s)) return rc;
   auto bf = [](const void* p) { return static_cast<__nv_bfloat16*>(const_cast<void*>(p)); };
@@ -715,22 +886,39 @@ extern "C" int mm_surrogate_forward(const mm_surrogate_desc* d, int check, void*
   if (int rc = pointwise<32>(d->xp, kWidth, d->wlb, S, d->err,
                              EpiLayer{d->params + off_bl(), nullptr, bf(d->hp[0]), bf(d->hc[0]), S, 0}, s))
     return rc;
+  // without pre-activation buffers (inference) the last layer's
+  // channel-major copy, only read by the backward pass, is skipped
+  const bool train = d->z[0] != nullptr;
   for (int l = 0; l < kLayers; ++l) {
     if (int rc = spectral(d->F, d->hc[l], d->v[l], S, d->err, s)) return rc;
-    mix_forward_kernel<<<dim3(kNModes, (S + 63) / 64), 256, 0, s>>>(d->v[l], d->params + off_rr(l),
-                                                                       d->params + off_ri(l), bf(d->voc), S);
-    MM_CHECK_LAUNCH("surrogate spectral mixing");
-    // without pre-activation buffers (inference) the last layer's
-    // channel-major copy, only read by the backward pass, is skipped too
-    const bool train = d->z[0] != nullptr;
+    if (int rc = mix_forward(d->v[l], d->params + off_rr(l), d->params + off_ri(l), bf(d->voc), S, s)) return rc;
     const EpiLayer epi{d->params + off_b(l), train ? d->z[l] : nullptr, bf(d->hp[l + 1]),
                        (train || l < kLayers - 1) ? bf(d->hc[l + 1]) : nullptr, S, l < kLayers - 1};
     if (int rc = fused(d->G, d->voc, d->hp[l], d->wb[l], S, d->err, epi, s)) return rc;
   }
-  if (int rc = pointwise<16>(d->hp[kLayers], kWidth, d->wpb, S, d->err,
-                             EpiProject{d->params + off_bp(), d->base, d->y, S}, s))
-    return rc;
+  if (planes) return pointwise<16>(d->hp[kLayers], kWidth, d->wpb, S, d->err,
+                                  EpiPlanes{d->params + off_bp(), d->base, planes, S}, s);
+  return pointwise<16>(d->hp[kLayers], kWidth, d->wpb, S, d->err, EpiProject{d->params + off_bp(), d->base, d->y, S},
+                       s);
+}
+}  // namespace
+}  // namespace mm
+
+extern "C" int mm_surrogate_forward(const mm_surrogate_desc* d, int check, void* stream) {
+  using namespace mm;
+  if (int rc = check_desc(d, false)) return rc;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (int rc = forward_pass(d, nullptr, s)) return rc;
   return finish(check, d->err, s, "surrogate forward");
+}
+
+extern "C" int mm_surrogate_predict(const mm_surrogate_desc* d, float* planes, int check, void* stream) {
+  using namespace mm;
+  if (int rc = check_desc(d, false)) return rc;
+  MM_CHECK_ARG(planes != nullptr, "NULL PSF planes");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (int rc = forward_pass(d, planes, s)) return rc;
+  return finish(check, d->err, s, "surrogate predict");
 }
 
 extern "C" int mm_surrogate_backward(const mm_surrogate_desc* d, const float* target, double* loss, int check,
@@ -821,8 +1009,8 @@ extern "C" int mm_surrogate_planes(const float* y, float* out, int sites, void* 
   using namespace mm;
   MM_CHECK_ARG(y && out && sites >= 1, "bad surrogate plane arguments");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  const long long m = (long long)sites * kPlanes * kPix;
-  psf_planes_kernel<<<(unsigned)((m + 255) / 256), 256, 0, s>>>(y, out, sites);
+  MM_CHECK_ARG(sites <= 65535, "surrogate planes: %d sites exceed one launch (65,535)", sites);
+  psf_planes_kernel<<<dim3(kPix / kPlanePixels, sites), kPlanePixels, 0, s>>>(y, out);
   MM_CHECK_LAUNCH("surrogate PSF planes");
   return MM_OK;
 }

@@ -256,7 +256,7 @@ class PSFSurrogate:
                 log(f"epoch {ep}: loss {history[-1]:.5f}")
         return history
 
-    def predict(self, xp, xc, *, batch=512):
+    def predict(self, xp, xc, *, batch=2048):
         """PSF planes (S, 9, 64, 64) FP32 (negatives clipped) for S sites."""
         import torch
         S = self._check_inputs(xp, xc)
@@ -264,9 +264,10 @@ class PSFSurrogate:
         xp3, xc3 = xp.view(S, NPIX, WIDTH), xc.view(S, WIDTH, NPIX)
         for s0 in range(0, S, batch):
             s1 = min(S, s0 + batch)
-            y = self.forward(xp3[s0:s1].reshape(-1, WIDTH), xc3[s0:s1].reshape(-1, NPIX), train=False)
-            _lib.check(_lib.load().mm_surrogate_planes(y.data_ptr(), out[s0:s1].data_ptr(), s1 - s0,
-                                                        _lib.stream_of(self.device)), "surrogate planes")
+            xpb, xcb = xp3[s0:s1].reshape(-1, WIDTH), xc3[s0:s1].reshape(-1, NPIX)
+            d, _ = self._desc(s1 - s0, xpb, xcb, train=False)
+            _lib.check(_lib.load().mm_surrogate_predict(d, out[s0:s1].data_ptr(), 0, _lib.stream_of(self.device)),
+                       "surrogate predict")
         return out
 
 

@@ -21,7 +21,7 @@ def _gemm(a, b, check=True):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("m,n,k", [(128, 32, 64), (300, 256, 4096), (576, 32, 4096), (4096, 32, 576),
-                                   (200, 16, 32), (130, 96, 80)])
+                                   (200, 16, 32), (130, 96, 80), (5120, 2048, 192)])
 def test_gemm_bf16_matches_fp32_product(m, n, k):
     import torch
     g = torch.Generator(device="cuda").manual_seed(m * 7 + n + k)
@@ -126,6 +126,31 @@ def test_surrogate_forward_and_gradients_match_fp64_oracle():
     gg = model.numpy_grads()
     errs = {k: rel_l2(gg[k], go[k]) for k in go}
     assert all(v < 5e-2 for v in errs.values()), errs
+
+
+@pytest.mark.gpu
+def test_surrogate_predict_planes():
+    """Inference writes the clipped PSF planes from the projection epilogue:
+    the same values as the training-path forward followed by the plane
+    reshuffle (FP32 sums in another order: 1e-6), and the FP64 definition
+    (2 %, as above) on 45 sites: a partial 8-site group and more layer tiles
+    (192) than SMs, so each persistent CTA reuses both accumulators."""
+    import torch
+    from maomi_b200 import _lib
+    from maomi_b200.surrogate import targets_to_planes
+    from oracle import surrogate as Sg
+    model, xp, xc, t, Xq, T = _model_and_batch(45, 6)
+    planes = model.predict(xp, xc).cpu().numpy()
+    y = model.forward(xp, xc, check=True, train=False)
+    ref = torch.empty((45, 9, 64, 64), dtype=torch.float32, device="cuda")
+    _lib.check(_lib.load().mm_surrogate_planes(y.data_ptr(), ref.data_ptr(), 45, _lib.stream_of("cuda")), "planes")
+    assert planes.shape == (45, 9, 64, 64) and planes.min() >= 0.0
+    assert rel_l2(planes, ref.cpu().numpy()) < 1e-6
+    p = model.numpy_params()
+    yo, _ = Sg.forward(p, Xq[:4], Sg.spectral_matrices())
+    po = np.maximum(targets_to_planes(torch.as_tensor(yo)).numpy(), 0.0)
+    base = np.maximum(targets_to_planes(torch.as_tensor(np.broadcast_to(p["base"], yo.shape).copy())).numpy(), 0.0)
+    assert rel_l2(planes[:4] - base, po - base) < 2e-2
 
 
 @pytest.mark.gpu
