@@ -256,7 +256,7 @@ class PSFSurrogate:
                 log(f"epoch {ep}: loss {history[-1]:.5f}")
         return history
 
-    def predict(self, xp, xc, *, batch=2048):
+    def predict(self, xp, xc, *, batch=8192):
         """PSF planes (S, 9, 64, 64) FP32 (negatives clipped) for S sites."""
         import torch
         S = self._check_inputs(xp, xc)
