@@ -252,6 +252,14 @@ size_t mm_propagate_workspace_size(const mm_stage_plan* plan, int slots, int sch
 int mm_propagate_sites(const mm_stage_plan* plan, int schedule, int slots, void* workspace,
                        size_t workspace_bytes, int check, void* stream);
 
+/* The check of mm_propagate_sites on its own: synchronise the stream and read
+ * the device error flag of a propagation that ran with check = 0 in
+ * `workspace` (same plan, schedule and slots), for example inside a replayed
+ * CUDA graph, where the call itself cannot synchronise.  Returns
+ * MM_ERR_ARGUMENT for out-of-range site windows, MM_ERR_TIMEOUT for a
+ * dependency wait that ran out. */
+int mm_propagate_status(const mm_stage_plan* plan, int schedule, int slots, const void* workspace, void* stream);
+
 /* Propagation for callers that cannot allocate device memory (no counterpart
  * in the reference).  Same work and outputs as mm_propagate_sites, with the
  * workspace taken from a fixed 32 MiB device array inside the library instead

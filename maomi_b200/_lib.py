@@ -133,6 +133,7 @@ SIGNATURES = {
     "mm_base_field": (c_int, [POINTER(BaseDesc), c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     "mm_propagate_workspace_size": (c_size_t, [POINTER(StagePlan), c_int, c_int]),
     "mm_propagate_sites": (c_int, [POINTER(StagePlan), c_int, c_int, c_void_p, c_size_t, c_int, c_void_p]),
+    "mm_propagate_status": (c_int, [POINTER(StagePlan), c_int, c_int, c_void_p, c_void_p]),
     "mm_propagate_sites_noalloc": (c_int, [POINTER(StagePlan), c_int, c_int, c_int, c_void_p]),
     "mm_items_blocks": (c_int, [c_int, c_int]),
     "mm_propagate_items_workspace_size": (c_size_t, [POINTER(ItemClass)]),

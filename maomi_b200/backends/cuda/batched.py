@@ -208,7 +208,12 @@ class OpticalPlan:
         import torch
         dev = self.device
         P = len(offsets)
-        off = _lib.upload(np.asarray(offsets, np.int32), dev)
+        if isinstance(offsets, torch.Tensor) and offsets.is_cuda:  # already on the device (graph capture)
+            if offsets.dtype != torch.int32 or tuple(offsets.shape) != (P, 2) or not offsets.is_contiguous():
+                raise ValueError("device offsets must be a contiguous (P, 2) int32 tensor")
+            off = offsets
+        else:
+            off = _lib.upload(np.asarray(offsets, np.int32), dev)
         zb = self.kernels[1].shape[0]
         fh, fw = self.focal_shape
         focal = torch.empty((P, zb, fh, fw), dtype=torch.float32, device=dev)
@@ -256,7 +261,8 @@ class OpticalPlan:
             events[1].record()
         _lib.check(rc, "propagation")
         self.paths_evaluated += P
-        return dict(focal=focal, images=imgs, profiles=prof, offsets=off, workspace=work)
+        return dict(focal=focal, images=imgs, profiles=prof, offsets=off, workspace=work, plan=plan, schedule=sched,
+                    slots=slots, workspace_base=base)
 
     def finalize_focal(self, focal, *, psf=True, sums=False):
         """(P,Z,h,w) focal powers -> psf (P,X,Y,Z), energies (P) and site sums."""
@@ -312,19 +318,61 @@ class OpticalPlan:
         return out
 
     def prepare_graph(self, batch_size=32):
-        """Kept for signature compatibility: the persistent launch already runs
-        every site in one kernel, so no per-batch graph is needed."""
+        """Capture the focal path of one fixed batch of ``batch_size`` sites
+        (queue reset, persistent propagation, focal finalize) in a CUDA graph
+        over a device offset buffer; evaluate_graph replays it with only the
+        offsets changed (batched.py:103-120)."""
+        import torch
         if not self.native:
             raise ValueError("Graph requires native gather without CPU indexing")
-        self.graphs.setdefault(batch_size, None)
+        batch_size = int(batch_size)
+        if batch_size < 1:
+            raise ValueError("batch_size must be >= 1")
+        if self.graphs.get(batch_size) is not None:
+            return
+        dev = self.device
+        buf = torch.zeros((batch_size, 2), dtype=torch.int32, device=dev)  # window (0, 0) is always valid
+        side = torch.cuda.Stream(device=dev)
+        side.wait_stream(torch.cuda.current_stream(dev))
+        with torch.cuda.stream(side), torch.inference_mode():
+            for _ in range(3):  # settles allocations and kernel attributes before capture
+                self.finalize_focal(self.run_sites(buf, tail_per_site=False, slots=batch_size)["focal"])
+        torch.cuda.current_stream(dev).wait_stream(side)
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph), torch.inference_mode():
+            run = self.run_sites(buf, tail_per_site=False, slots=batch_size, check=False)
+            psf, _, _, _ = self.finalize_focal(run["focal"])
+        self.paths_evaluated -= 4 * batch_size  # warm-up and capture evaluated no caller's sites
+        host = torch.zeros((batch_size, 2), dtype=torch.int32, pin_memory=True)
+        self.graphs[batch_size] = dict(graph=graph, offsets=buf, host=host, psf=psf, run=run)
 
     def evaluate_graph(self, points_um, *, batch_size=32):
-        """Focal-only evaluation (batched.py:121-146 schema)."""
+        """Focal-only evaluation by graph replay, ``batch_size`` sites per
+        replay with the last batch padded by window (0, 0) sites
+        (batched.py:121-146 schema)."""
+        import torch
         self.prepare_graph(batch_size)
-        out = self.evaluate(points_um, batch_size=batch_size, tails=False)
-        pts = out["points_um"]
-        out["graph_padding_slots"] = int(np.ceil(len(pts) / batch_size)) * batch_size - len(pts)
-        return out
+        g = self.graphs[int(batch_size)]
+        pts, off = self.offsets(points_um)
+        off = np.asarray(off, np.int32).reshape(-1, 2)
+        run = g["run"]
+        collected = []
+        with torch.inference_mode():
+            for s0 in range(0, len(pts), batch_size):
+                part = off[s0:s0 + batch_size]
+                g["host"].zero_()
+                g["host"][:len(part)] = torch.from_numpy(part)
+                g["offsets"].copy_(g["host"], non_blocking=True)
+                g["graph"].replay()
+                _lib.check(_lib.load().mm_propagate_status(run["plan"], run["schedule"], run["slots"],
+                                                           _lib.c_void_p(run["workspace_base"]),
+                                                           _lib.stream_of(self.device)), "propagation")
+                collected.append(g["psf"][:len(part)].cpu().numpy().copy())
+                self.paths_evaluated += len(part)
+        X, Y = self.focal_resample.shape
+        psfs = np.concatenate(collected) if collected else np.zeros((0, X, Y, self.kernels[1].shape[0]), np.float32)
+        return {"psfs": psfs, "points_um": pts, "tails_computed": False,
+                "graph_padding_slots": int(np.ceil(len(pts) / batch_size)) * batch_size - len(pts)}
 
     def cached(self, points_um, *, batch_size=16):
         pts, off = self.offsets(points_um)

@@ -637,6 +637,28 @@ extern "C" size_t mm_propagate_workspace_size(const mm_stage_plan* plan, int slo
   return mm::carve(nullptr, plan->n, plan->n2, slots).bytes;
 }
 
+extern "C" int mm_propagate_status(const mm_stage_plan* plan, int schedule, int slots, const void* workspace,
+                                   void* stream) {
+  using namespace mm;
+  MM_CHECK_ARG(plan != nullptr && workspace != nullptr && slots >= 1, "bad propagation status arguments");
+  MM_CHECK_ARG(schedule == MM_SCHEDULE_PERSISTENT || schedule == MM_SCHEDULE_BATCHED, "unknown schedule %d", schedule);
+  MM_CHECK_ARG(reinterpret_cast<uintptr_t>(workspace) % 256 == 0, "workspace must be 256-byte aligned");
+  const Workspace w =
+      carve(const_cast<void*>(workspace), plan->n, plan->n2, propagation_slots(plan->nsites, slots, schedule));
+  MM_CHECK_CUDA(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)), "propagation");
+  int err = 0;
+  MM_CHECK_CUDA(cudaMemcpy(&err, w.error, sizeof(int), cudaMemcpyDeviceToHost), "read error flag");
+  if (err & 2) {
+    set_error("a site window lies outside the screen volume (offsets out of range)");
+    return MM_ERR_ARGUMENT;
+  }
+  if (err) {
+    set_error("persistent propagation: a dependency wait timed out");
+    return MM_ERR_TIMEOUT;
+  }
+  return MM_OK;
+}
+
 extern "C" int mm_propagate_sites(const mm_stage_plan* plan, int schedule, int slots, void* workspace,
                                   size_t workspace_bytes, int check, void* stream) {
   using namespace mm;

@@ -77,6 +77,29 @@ def test_evaluate_per_site_matches_oracle(small):
     assert plan.paths_evaluated == len(d["points"])
 
 
+def test_evaluate_graph_replays_a_captured_focal_batch(small):
+    """prepare_graph / evaluate_graph (reference batched.py:103-146): the focal
+    path of a fixed 4-site batch is captured once in a CUDA graph and replayed
+    per chunk of the 9 sites, the last chunk padded with window (0, 0) sites.
+    The PSFs equal evaluate's bit for bit (same kernels on the same inputs),
+    the padding is reported, only the caller's sites are counted, and a second
+    call reuses the captured graph."""
+    from maomi_b200.backends.cuda.batched import OpticalPlan
+    d, cfg, raw = small
+    plan = OpticalPlan(cfg, raw)
+    ref = OpticalPlan(cfg, raw).evaluate(d["points"], batch_size=4)
+    out = plan.evaluate_graph(d["points"], batch_size=4)
+    assert out["graph_padding_slots"] == 3 and out["tails_computed"] is False
+    np.testing.assert_array_equal(out["psfs"], ref["psfs"])
+    graph = plan.graphs[4]["graph"]
+    again = plan.evaluate_graph(d["points"][::-1], batch_size=4)
+    assert plan.graphs[4]["graph"] is graph
+    np.testing.assert_array_equal(again["psfs"], ref["psfs"][::-1])
+    assert plan.paths_evaluated == 2 * len(d["points"])
+    with pytest.raises(ValueError, match="Outside FOV"):
+        plan.evaluate_graph([[-1.0, 0.0]], batch_size=4)
+
+
 @pytest.fixture(scope="module")
 def bench_sites():
     from oracle import optics as O
