@@ -444,12 +444,17 @@ int mm_gemm_bf16_tn(const void* a, const void* b, float* d, int m, int n, int k,
  *   base (4096,16) FP32 mean PSF added to the projection
  *   xp (S*4096,32) / xc (S*32,4096) inputs; hp[l]/hc[l] (l = 0..4) activations, same shapes
  *   z[l] (S,4096,32) FP32 pre-activations (l = 0..2 needed for backward)
- *   v[l] (S,576,32) FP32 spectral coefficients; voc (S*32,576) BF16 scratch
+ *   v[l] (S,576,32) FP32 spectral coefficients (written only when z[0] is
+ *   set: the mixing backward reads them); voc (S*32,576) BF16 scratch
  *   y (S,4096,16) FP32 prediction (planes 0..8 used)
  *   backward: dyp (S*4096,16), dyc (S*16,4096), dzp[2] (S*4096,32), dzc[2]
  *   (S*32,4096) BF16; dvo (S,576,32) FP32; dvc (S*32,576) BF16
  *   err: zeroed device int (bit 1: site off the input grid, bit 4: a
  *   tensor-core pipeline wait timed out)
+ *   vb (288,S,64) BF16 spectral coefficients mode-major (row (q, s): the
+ *   re and im rows of mode q, 32 channels each), the tensor-core mixing's A
+ *   mixb[l] (288*64,64) BF16 per-mode mixing operators (filled from Rr/Ri by
+ *   the forward pass; row 64 q + 2 o + c, c = 0 real / 1 imaginary output)
  */
 typedef struct {
   int sites;
@@ -480,6 +485,8 @@ typedef struct {
   float* dvo;
   void* dvc;
   int* err;
+  void* vb;
+  void* mixb[4];
 } mm_surrogate_desc;
 
 /* Offsets (floats) of Wl, bl, {W_l, b_l, Rr_l, Ri_l} for l = 0..3, Wp, bp and the total (21 entries). */

@@ -95,7 +95,7 @@ class SurrogateDesc(ctypes.Structure):
                 ("hc", c_void_p * 5), ("z", c_void_p * 4), ("v", c_void_p * 4),
                 ("voc", c_void_p), ("y", c_void_p), ("dyp", c_void_p), ("dyc", c_void_p),
                 ("dzp", c_void_p * 2), ("dzc", c_void_p * 2), ("dvo", c_void_p),
-                ("dvc", c_void_p), ("err", c_void_p)]
+                ("dvc", c_void_p), ("err", c_void_p), ("vb", c_void_p), ("mixb", c_void_p * 4)]
 
 
 # name -> (restype, argtypes)

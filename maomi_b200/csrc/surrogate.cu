@@ -131,16 +131,35 @@ __global__ void spectral_constants_kernel(__nv_bfloat16* F, __nv_bfloat16* G, __
 }
 
 // ---------------------------------------------------------------- epilogues
-// V / dVo: rows of the spectral GEMM (mode rows) x (8 sites x 32 channels).
+// V / dVo: rows of the spectral GEMM (mode rows) x (8 sites x 32 channels),
+// FP32 (S, 576, 32) into `out` and / or BF16 mode-major (288, S, 64) into
+// `vb` (row (q, s) = the re row then the im row of mode q); either may be NULL.
 struct EpiSpectral {
-  float* out;  // (S, 576, 32)
+  float* out;
+  __nv_bfloat16* vb;
   int sites;
   __device__ void store(int bx, int by, int row, int c, const float (&v)[32], unsigned char* scratch) const {
     const int r = bx * gemm::kBM + row, s = by * kGroup + c / kWidth;
     if (r >= kRows || s >= sites) return;
-    float4* dst = reinterpret_cast<float4*>(out + ((size_t)s * kRows + r) * kWidth);
+    if (out) {
+      float4* dst = reinterpret_cast<float4*>(out + ((size_t)s * kRows + r) * kWidth);
 #pragma unroll
-    for (int k = 0; k < 8; ++k) dst[k] = make_float4(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3]);
+      for (int k = 0; k < 8; ++k) dst[k] = make_float4(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3]);
+    }
+    if (vb) {
+      uint4* dst = reinterpret_cast<uint4*>(vb + (((size_t)(r >> 1) * sites + s) * 2 + (r & 1)) * kWidth);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        __nv_bfloat162 a = __floats2bfloat162_rn(v[8 * k], v[8 * k + 1]), b = __floats2bfloat162_rn(v[8 * k + 2], v[8 * k + 3]);
+        __nv_bfloat162 e = __floats2bfloat162_rn(v[8 * k + 4], v[8 * k + 5]), f = __floats2bfloat162_rn(v[8 * k + 6], v[8 * k + 7]);
+        uint4 u;
+        u.x = *reinterpret_cast<uint32_t*>(&a);
+        u.y = *reinterpret_cast<uint32_t*>(&b);
+        u.z = *reinterpret_cast<uint32_t*>(&e);
+        u.w = *reinterpret_cast<uint32_t*>(&f);
+        dst[k] = u;
+      }
+    }
   }
 };
 
@@ -335,102 +354,9 @@ struct EpiWeightGrad {
 };
 
 // ------------------------------------------------------- spectral mixing
-// Vo_q = V_q R_q (complex, per mode): V (S, 576, 32) FP32 -> Voc (S*32, 576) BF16.
-//
-// A block owns 8 consecutive modes q0..q0+7 and walks the groups of
-// kMixStage sites g = blockIdx.y, blockIdx.y + gridDim.y, ... (one resident
-// wave of blocks).  Thread (m, o) = (lane % 8, 4 * warp + lane / 8) keeps
-// column o of R_{q0+m} (32 complex weights) in registers, so the inner loop
-// reads only the staged V rows (float4 loads, conflict-free with a 36-float
-// row pitch); the next group's rows are loaded into registers while the
-// current group is mixed, and every store of a warp covers four whole
-// 32-byte segments of Voc (8 modes x re/im of one (site, channel) row).
-constexpr int kMixModes = 8, kMixStage = 8, kMixPitch = 36;
-
-__global__ void __launch_bounds__(256) mix_forward_kernel(const float* __restrict__ V, const float* __restrict__ Rr,
-                                                          const float* __restrict__ Ri, __nv_bfloat16* __restrict__ Voc,
-                                                          int sites) {
-  __shared__ __align__(16) float vr[kMixStage][kMixModes][kMixPitch];
-  __shared__ __align__(16) float vi[kMixStage][kMixModes][kMixPitch];
-  const int t = threadIdx.x, lane = t & 31, m = lane & 7, o = 4 * (t >> 5) + (lane >> 3);
-  const int q0 = blockIdx.x * kMixModes, q = q0 + m;
-  const int groups = (sites + kMixStage - 1) / kMixStage;
-  // staged float4 f = t + 256 k of a group: site f / 128, row (f / 8) % 16, column quad f % 8
-  auto load_group = [&](int gi, float4 (&r)[4]) {
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      const int f = t + 256 * k, s = gi * kMixStage + (f >> 7), row = (f >> 3) & 15, c4 = f & 7;
-      r[k] = s < sites ? __ldg(reinterpret_cast<const float4*>(V + ((size_t)s * kRows + 2 * q0 + row) * kWidth) + c4)
-                       : make_float4(0.f, 0.f, 0.f, 0.f);
-    }
-  };
-  float4 pre[4];
-  if (blockIdx.y < groups) load_group(blockIdx.y, pre);
-  float wr[32], wi[32];
-#pragma unroll
-  for (int i = 0; i < 32; ++i) {
-    wr[i] = __ldg(Rr + (size_t)q * 1024 + i * 32 + o);
-    wi[i] = __ldg(Ri + (size_t)q * 1024 + i * 32 + o);
-  }
-  for (int gi = blockIdx.y; gi < groups; gi += gridDim.y) {
-    __syncthreads();  // the previous group's rows have been read
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      const int f = t + 256 * k, sl = f >> 7, row = (f >> 3) & 15, c4 = f & 7;
-      float* dst = (row & 1) ? &vi[sl][row >> 1][4 * c4] : &vr[sl][row >> 1][4 * c4];
-      *reinterpret_cast<float4*>(dst) = pre[k];
-    }
-    __syncthreads();
-    if (gi + (int)gridDim.y < groups) load_group(gi + gridDim.y, pre);  // in flight during the mixing below
-    const int s0 = gi * kMixStage;
-    // two sites at a time (four independent FMA chains); rows of sites past
-    // the end were staged as zeros and their results are not stored
-#pragma unroll 1
-    for (int sl = 0; sl < kMixStage; sl += 2) {
-      float re0 = 0.f, im0 = 0.f, re1 = 0.f, im1 = 0.f;
-#pragma unroll
-      for (int i4 = 0; i4 < 8; ++i4) {
-        const float4 a0 = *reinterpret_cast<const float4*>(&vr[sl][m][4 * i4]);
-        const float4 b0 = *reinterpret_cast<const float4*>(&vi[sl][m][4 * i4]);
-        const float4 a1 = *reinterpret_cast<const float4*>(&vr[sl + 1][m][4 * i4]);
-        const float4 b1 = *reinterpret_cast<const float4*>(&vi[sl + 1][m][4 * i4]);
-        const float x0[4] = {a0.x, a0.y, a0.z, a0.w}, y0[4] = {b0.x, b0.y, b0.z, b0.w};
-        const float x1[4] = {a1.x, a1.y, a1.z, a1.w}, y1[4] = {b1.x, b1.y, b1.z, b1.w};
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          const int i = 4 * i4 + j;
-          re0 = fmaf(x0[j], wr[i], fmaf(-y0[j], wi[i], re0));
-          im0 = fmaf(x0[j], wi[i], fmaf(y0[j], wr[i], im0));
-          re1 = fmaf(x1[j], wr[i], fmaf(-y1[j], wi[i], re1));
-          im1 = fmaf(x1[j], wi[i], fmaf(y1[j], wr[i], im1));
-        }
-      }
-      const int s = s0 + sl;
-      if (s < sites)
-        *reinterpret_cast<__nv_bfloat162*>(Voc + ((size_t)s * kWidth + o) * kRows + 2 * q) =
-            __floats2bfloat162_rn(re0, im0);
-      if (s + 1 < sites)
-        *reinterpret_cast<__nv_bfloat162*>(Voc + ((size_t)(s + 1) * kWidth + o) * kRows + 2 * q) =
-            __floats2bfloat162_rn(re1, im1);
-    }
-  }
-}
-
-// One resident wave of mixing blocks: 36 mode groups x as many site-group
-// walkers as fit beside them.
-int mix_forward(const float* V, const float* Rr, const float* Ri, __nv_bfloat16* Voc, int S, cudaStream_t s) {
-  int device = 0, sms = 0, per_sm = 0;
-  MM_CHECK_CUDA(cudaGetDevice(&device), "cudaGetDevice");
-  MM_CHECK_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "SM count");
-  MM_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, mix_forward_kernel, 256, 0), "occupancy(mix)");
-  const int groups = (S + kMixStage - 1) / kMixStage;
-  const int walkers = std::max(1, std::min(groups, sms * std::max(per_sm, 1) / (kNModes / kMixModes)));
-  mix_forward_kernel<<<dim3(kNModes / kMixModes, walkers), 256, 0, s>>>(V, Rr, Ri, Voc, S);
-  MM_CHECK_LAUNCH("surrogate spectral mixing");
-  return MM_OK;
-}
-
-// Backward of the mixing for one mode over all sites: dV (-> dVc BF16) and dR.
+// The forward mixing Vo_q = V_q R_q runs on the tensor cores (mix_tc_kernel
+// below).  Backward of the mixing for one mode over all sites: dV (-> dVc
+// BF16) and dR, from the FP32 coefficients the training forward keeps.
 __global__ void __launch_bounds__(256) mix_backward_kernel(const float* __restrict__ V, const float* __restrict__ dVo,
                                                            const float* __restrict__ Rr, const float* __restrict__ Ri,
                                                            __nv_bfloat16* __restrict__ dVc, float* __restrict__ dRr,
@@ -605,6 +531,22 @@ __global__ void weights_bf16_kernel(WeightPtrs w) {
   }
 }
 
+// Per-mode mixing operators as tensor-core B operands (K-major BF16): for
+// mode q, output n = 2 o + c (c = 0 real, 1 imaginary) and input k = 32 c' + i
+// (the re then the im row of V_q), B[64 q + n][k] is the coefficient of input
+// k in output n of Vo_q = V_q R_q:
+//   re_o = sum_i Re(V_i) Rr_io - Im(V_i) Ri_io,  im_o = sum_i Re(V_i) Ri_io + Im(V_i) Rr_io.
+__global__ void mix_operators_kernel(const float* __restrict__ Rr, const float* __restrict__ Ri,
+                                     __nv_bfloat16* __restrict__ B) {
+  const int q = blockIdx.x;
+  for (int e = threadIdx.x; e < 64 * 64; e += blockDim.x) {
+    const int n = e >> 6, k = e & 63, o = n >> 1, c = n & 1, ci = k >> 5, i = k & 31;
+    const float rr = Rr[(size_t)q * 1024 + i * 32 + o], ri = Ri[(size_t)q * 1024 + i * 32 + o];
+    const float w = c == 0 ? (ci == 0 ? rr : -ri) : (ci == 0 ? ri : rr);
+    B[(size_t)q * 4096 + e] = __float2bfloat16_rn(w);
+  }
+}
+
 // ------------------------------------------------------------------ inputs
 // pooled[g][X][Y] = scale/16 * sum over the group's screens and the 4x4 block.
 struct PoolArgs {
@@ -677,6 +619,121 @@ __global__ void __launch_bounds__(kPlanePixels) psf_planes_kernel(const float* _
 }
 
 
+// ------------------------------------------- spectral mixing on tensor cores
+// Vo_q = V_q R_q for 8 modes q0..q0+7 of 128 sites per CTA: per mode one
+// 128 x 64 x 64 BF16 MMA, A = the sites' mode-major rows (vb rows q S + s,
+// [re | im] of V_q), B = the mode's operator (mixb rows 64 q ..), into TMEM
+// columns 64 (q - q0) + 2 o + c.  All 8 modes' operands land in shared memory
+// at once (8 x 24 KB, one mbarrier); one thread issues the 32 MMAs, then the
+// four warps read, per group of 4 channels, the 8 modes' (re, im) pairs and
+// write each (site, channel) row's 16 values as one 32-byte segment of Voc.
+// Waits are bounded (bit 4 of *err); a failed CTA stores nothing.
+constexpr int kMixTcModes = 8;
+constexpr int kMixTcATile = 128 * 64 * 2, kMixTcBTile = 64 * 64 * 2;
+constexpr size_t kMixTcSmem = 1024 + (size_t)kMixTcModes * (kMixTcATile + kMixTcBTile) + 64;
+
+__global__ void __launch_bounds__(128, 1)
+    mix_tc_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
+                  __nv_bfloat16* __restrict__ Voc, int sites, int* err) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  unsigned char* a_tiles = base;
+  unsigned char* b_tiles = base + kMixTcModes * kMixTcATile;
+  uint64_t* full = reinterpret_cast<uint64_t*>(b_tiles + kMixTcModes * kMixTcBTile);
+  uint64_t* done = full + 1;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+  __shared__ int s_fail;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int s0 = blockIdx.x * 128, q0 = blockIdx.y * kMixTcModes;
+  if (threadIdx.x == 0) {
+    umma::mbar_init(full, 1);
+    umma::mbar_init(done, 1);
+    umma::fence_barrier_init();
+    s_fail = 0;
+    umma::prefetch_map(&mapA);
+    umma::prefetch_map(&mapB);
+  }
+  if (warp == 0) umma::tmem_alloc(tmem_slot, 512);
+  umma::fence_before_sync();
+  __syncthreads();
+  umma::fence_after_sync();
+  const uint32_t tmem = *tmem_slot;
+  if (threadIdx.x == 0) {
+    umma::mbar_arrive_expect_tx(full, kMixTcModes * (kMixTcATile + kMixTcBTile));
+    for (int i = 0; i < kMixTcModes; ++i) {
+      umma::tma_load_2d(a_tiles + i * kMixTcATile, &mapA, full, 0, (q0 + i) * sites + s0);
+      umma::tma_load_2d(b_tiles + i * kMixTcBTile, &mapB, full, 0, (q0 + i) * 64);
+    }
+    if (umma::mbar_wait(full, 0, gemm::kWaitLimit)) {
+      umma::fence_after_sync();
+      for (int i = 0; i < kMixTcModes; ++i) {
+        const uint64_t da = umma::sw128_desc(a_tiles + i * kMixTcATile), db = umma::sw128_desc(b_tiles + i * kMixTcBTile);
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+          umma::mma_bf16(tmem + i * 64, da + 2 * k, db + 2 * k, umma::idesc_bf16(128, 64), k > 0 ? 1u : 0u);
+      }
+    } else {
+      atomicOr(err, 16);
+      s_fail = 1;
+    }
+    umma::mma_commit(done);  // arrives once the MMAs above (if any) have run
+  }
+  __syncwarp();
+  bool ok = umma::mbar_wait(done, 0, gemm::kWaitLimit);
+  if (!ok) atomicOr(err, 16);
+  __syncthreads();  // s_fail is final
+  ok = __all_sync(0xffffffffu, ok && !s_fail);
+  umma::fence_after_sync();
+  if (ok) {
+    const int row = warp * 32 + lane, s = s0 + row;
+    const uint32_t lane_addr = tmem + (uint32_t(warp * 32) << 16);
+    for (int ob = 0; ob < kWidth / 4; ++ob) {  // channels 4 ob .. 4 ob + 3
+      float v[kMixTcModes][8];
+#pragma unroll
+      for (int i = 0; i < kMixTcModes; ++i) umma::tmem_ld8(lane_addr + i * 64 + ob * 8, v[i]);
+      if (s < sites) {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          uint32_t w[kMixTcModes];
+#pragma unroll
+          for (int i = 0; i < kMixTcModes; ++i) {
+            __nv_bfloat162 h = __floats2bfloat162_rn(v[i][2 * j], v[i][2 * j + 1]);
+            w[i] = *reinterpret_cast<uint32_t*>(&h);
+          }
+          uint4* dst = reinterpret_cast<uint4*>(Voc + ((size_t)s * kWidth + 4 * ob + j) * kRows + 2 * q0);
+          dst[0] = make_uint4(w[0], w[1], w[2], w[3]);
+          dst[1] = make_uint4(w[4], w[5], w[6], w[7]);
+        }
+      }
+    }
+  }
+  umma::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) {
+    umma::fence_after_sync();
+    umma::tmem_dealloc(tmem, 512);
+  }
+}
+
+int mix_tc(const void* vb, const void* mixb, __nv_bfloat16* Voc, int S, int* err, cudaStream_t s) {
+  CUtensorMap ma, mb;
+  if (int rc = bf16_map(&ma, vb, (long long)kNModes * S, 64, 128)) return rc;
+  if (int rc = bf16_map(&mb, mixb, (long long)kNModes * 64, 64, 64)) return rc;
+  MM_CHECK_ARG((long long)kNModes * S < (1ll << 31), "mixing: %d sites exceed the row index range", S);
+  MM_CHECK_CUDA(cudaFuncSetAttribute(mix_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMixTcSmem),
+                "cudaFuncSetAttribute(mix)");
+  int per_sm = 0;
+  MM_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, mix_tc_kernel, 128, kMixTcSmem),
+                "occupancy(mix)");
+  if (per_sm != 1) {  // two CTAs of 512 tensor-memory columns would not fit on one SM
+    set_error("tensor-core mixing: %d CTAs per SM would not fit tensor memory", per_sm);
+    return MM_ERR_UNSUPPORTED;
+  }
+  mix_tc_kernel<<<dim3((S + 127) / 128, kNModes / kMixTcModes), 128, kMixTcSmem, s>>>(ma, mb, Voc, S, err);
+  MM_CHECK_LAUNCH("tensor-core spectral mixing");
+  return MM_OK;
+}
+
 // ------------------------------------------------------------ host side --
 // Flat FP32 parameter layout: Wl (32x32), bl (32), per layer W (32x32), b (32),
 // Rr (288x32x32), Ri (288x32x32), then Wp (16x32), bp (16).
@@ -696,7 +753,7 @@ struct Maps {
 };
 
 // Wide spectral GEMM: out (S, 576, 32) = A (576 x 4096) * act_c (S*32 x 4096)^T per site.
-int spectral(const void* A, const void* act_c, float* out, int S, int* err, cudaStream_t s) {
+int spectral(const void* A, const void* act_c, float* out, __nv_bfloat16* vb, int S, int* err, cudaStream_t s) {
   Maps m;
   if (int rc = bf16_map(&m.a, A, kRows, kPix, gemm::kBM)) return rc;
   if (int rc = bf16_map(&m.b, act_c, (long long)S * kWidth, kPix, 256)) return rc;
@@ -707,7 +764,7 @@ int spectral(const void* A, const void* act_c, float* out, int S, int* err, cuda
   t.ncols = 256;
   t.err = err;
   const dim3 grid((kRows + gemm::kBM - 1) / gemm::kBM, (S + kGroup - 1) / kGroup);
-  return launch_gemm<256, 32>(m.a, m.b, m.a, m.b, t, grid, EpiSpectral{out, S}, s);
+  return launch_gemm<256, 32>(m.a, m.b, m.a, m.b, t, grid, EpiSpectral{out, vb, S}, s);
 }
 
 // Fused layer GEMM: acc[pix, (site, o)] = A (4096 x 576) * coef_c (S*32 x 576)^T
@@ -781,6 +838,11 @@ int refresh_weights(const mm_surrogate_desc* d, cudaStream_t s) {
   w.wptb = static_cast<__nv_bfloat16*>(d->wptb);
   weights_bf16_kernel<<<4, 256, 0, s>>>(w);
   MM_CHECK_LAUNCH("surrogate weight copies");
+  for (int l = 0; l < kLayers; ++l) {
+    mix_operators_kernel<<<kNModes, 256, 0, s>>>(d->params + off_rr(l), d->params + off_ri(l),
+                                                  static_cast<__nv_bfloat16*>(d->mixb[l]));
+    MM_CHECK_LAUNCH("surrogate mixing operators");
+  }
   return MM_OK;
 }
 
@@ -790,7 +852,9 @@ int check_desc(const mm_surrogate_desc* d, bool backward) {
   MM_CHECK_ARG(d->F && d->G && d->params && d->base && d->xp && d->xc && d->voc && d->y && d->err && d->wlb &&
                    d->wpb && d->wptb,
                "surrogate descriptor has NULL buffers");
-  for (int l = 0; l < kLayers; ++l) MM_CHECK_ARG(d->wb[l] && d->wtb[l] && d->v[l], "layer %d buffers missing", l);
+  MM_CHECK_ARG(d->vb, "surrogate descriptor has no mode-major coefficient buffer");
+  for (int l = 0; l < kLayers; ++l)
+    MM_CHECK_ARG(d->wb[l] && d->wtb[l] && d->v[l] && d->mixb[l], "layer %d buffers missing", l);
   for (int l = 0; l <= kLayers; ++l) MM_CHECK_ARG(d->hp[l] && d->hc[l], "activation %d buffers missing", l);
   if (backward) {
     MM_CHECK_ARG(d->FT && d->GT && d->grads && d->dyp && d->dyc && d->dzp[0] && d->dzp[1] && d->dzc[0] && d->dzc[1] &&
@@ -886,12 +950,13 @@ int forward_pass(const mm_surrogate_desc* d, float* planes, cudaStream_t s) {
   if (int rc = pointwise<32>(d->xp, kWidth, d->wlb, S, d->err,
                              EpiLayer{d->params + off_bl(), nullptr, bf(d->hp[0]), bf(d->hc[0]), S, 0}, s))
     return rc;
-  // without pre-activation buffers (inference) the last layer's
-  // channel-major copy, only read by the backward pass, is skipped
+  // without pre-activation buffers (inference) the FP32 spectral
+  // coefficients and the last layer's channel-major copy, read only by the
+  // backward pass, are skipped
   const bool train = d->z[0] != nullptr;
   for (int l = 0; l < kLayers; ++l) {
-    if (int rc = spectral(d->F, d->hc[l], d->v[l], S, d->err, s)) return rc;
-    if (int rc = mix_forward(d->v[l], d->params + off_rr(l), d->params + off_ri(l), bf(d->voc), S, s)) return rc;
+    if (int rc = spectral(d->F, d->hc[l], train ? d->v[l] : nullptr, bf(d->vb), S, d->err, s)) return rc;
+    if (int rc = mix_tc(d->vb, d->mixb[l], bf(d->voc), S, d->err, s)) return rc;
     const EpiLayer epi{d->params + off_b(l), train ? d->z[l] : nullptr, bf(d->hp[l + 1]),
                        (train || l < kLayers - 1) ? bf(d->hc[l + 1]) : nullptr, S, l < kLayers - 1};
     if (int rc = fused(d->G, d->voc, d->hp[l], d->wb[l], S, d->err, epi, s)) return rc;
@@ -944,7 +1009,7 @@ extern "C" int mm_surrogate_backward(const mm_surrogate_desc* d, const float* ta
     bias_grad_kernel<<<(rows * 32 + 255) / 256, 256, 0, s>>>(bf(d->dzc[cur]), g + off_b(l), rows);
     MM_CHECK_LAUNCH("surrogate bias gradient");
     if (int rc = weight_grad<32>(d->dzc[cur], d->hc[l], g + off_w(l), S, d->err, s)) return rc;
-    if (int rc = spectral(d->GT, d->dzc[cur], d->dvo, S, d->err, s)) return rc;
+    if (int rc = spectral(d->GT, d->dzc[cur], d->dvo, nullptr, S, d->err, s)) return rc;
     mix_backward_kernel<<<kNModes, 256, 0, s>>>(d->v[l], d->dvo, d->params + off_rr(l), d->params + off_ri(l),
                                                bf(d->dvc), g + off_rr(l), g + off_ri(l), S);
     MM_CHECK_LAUNCH("surrogate mixing backward");

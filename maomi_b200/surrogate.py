@@ -98,6 +98,7 @@ class PSFSurrogate:
         self.wlb = torch.empty((WIDTH, WIDTH), dtype=bf, device=dev)
         self.wpb = torch.empty((OUT, WIDTH), dtype=bf, device=dev)
         self.wptb = torch.empty((WIDTH, OUT), dtype=bf, device=dev)
+        self.mixb = [torch.empty((NROWS // 2 * 64, 64), dtype=bf, device=dev) for _ in range(LAYERS)]
         self.err = torch.zeros(1, dtype=torch.int32, device=dev)
         self.loss_buf = torch.zeros(1, dtype=torch.float64, device=dev)
         self._bufs = {}
@@ -154,6 +155,7 @@ class PSFSurrogate:
             z=[torch.empty((S, NPIX, WIDTH), dtype=f32, device=dev) for _ in range(LAYERS - 1)],
             v=[torch.empty((S, NROWS, WIDTH), dtype=f32, device=dev) for _ in range(LAYERS)],
             voc=torch.empty((S * WIDTH, NROWS), dtype=bf, device=dev),
+            vb=torch.empty((NROWS // 2, S, 64), dtype=bf, device=dev),
             y=torch.empty((S, NPIX, OUT), dtype=f32, device=dev),
             dyp=torch.empty((S * NPIX, OUT), dtype=bf, device=dev),
             dyc=torch.empty((S * OUT, NPIX), dtype=bf, device=dev),
@@ -185,6 +187,9 @@ class PSFSurrogate:
             d.dzp[k], d.dzc[k] = b["dzp"][k].data_ptr(), b["dzc"][k].data_ptr()
         d.dvo, d.dvc = b["dvo"].data_ptr(), b["dvc"].data_ptr()
         d.err = self.err.data_ptr()
+        d.vb = b["vb"].data_ptr()
+        for l in range(LAYERS):
+            d.mixb[l] = self.mixb[l].data_ptr()
         return d, b
 
     @staticmethod
