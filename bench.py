@@ -274,8 +274,10 @@ def _timed(fn, steps, warmup, stream):
 
 # Tensor-core FLOPs of one site through the surrogate: lifting 2*4096*32*32,
 # per layer spectral 2*576*4096*32 + inverse 2*4096*576*32 + pointwise
-# 2*4096*32*32, projection 2*4096*32*16.
-SURROGATE_FLOPS_PER_SITE = 2 * 4096 * 32 * 32 + 4 * (2 * 2 * 576 * 4096 * 32 + 2 * 4096 * 32 * 32) + 2 * 4096 * 32 * 16
+# 2*4096*32*32 + mixing 288 modes x 8*32*32 (complex 32 x 32 products),
+# projection 2*4096*32*16.
+SURROGATE_FLOPS_PER_SITE = (2 * 4096 * 32 * 32 + 4 * (2 * 2 * 576 * 4096 * 32 + 2 * 4096 * 32 * 32 + 288 * 8 * 32 * 32)
+                            + 2 * 4096 * 32 * 16)
 
 
 def run_surrogate(args):
