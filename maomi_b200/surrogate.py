@@ -374,7 +374,13 @@ def rel_l2_per_site(a, b):
 class SurrogateStage:
     """Surrogate PSFs for every site, gated by the plain propagator on a seeded
     fraction of the sites (whole output replaced by the plain result when the
-    sample's relative L2 error exceeds ``tolerance``)."""
+    sample's relative L2 error exceeds ``tolerance``).
+
+    The gate runs first, on its sites only (their inputs, their predictions
+    and their plain PSFs); the surrogate runs on every site only after the
+    gate passes.  A failed gate keeps the gate sites' plain PSFs and
+    propagates the remaining sites.  Each site's prediction and plain PSF
+    depend on that site alone, so both orders give the same output."""
 
     def __init__(self, model, *, gate_fraction=0.05, tolerance=0.01, seed=0):
         self.model = model
@@ -395,18 +401,25 @@ class SurrogateStage:
             from .backends.cuda.batched import OpticalPlan
             plan = OpticalPlan(surrogate_config(config), raw_dev, device=dev)
         pts, off = plan.offsets(points_um)
-        xp, xc, _ = site_inputs(raw_dev, off, scale=self.model.input_scale, device=dev)
-        psfs = self.model.predict(xp, xc)
         gate = self.gate_sites(len(pts))
+        xg, xcg, _ = site_inputs(raw_dev, off[gate], scale=self.model.input_scale, device=dev)
+        predicted = self.model.predict(xg, xcg)
         t_gate, _, _ = plain_targets(config, raw_dev, pts[gate], device=dev, plan=plan)
         ref = targets_to_planes(t_gate)
-        per_site = rel_l2_per_site(psfs[torch.as_tensor(gate, device=dev)], ref)
-        sample = float(rel_l2_per_site(psfs[torch.as_tensor(gate, device=dev)].reshape(1, -1), ref.reshape(1, -1))[0])
+        per_site = rel_l2_per_site(predicted, ref)
+        sample = float(rel_l2_per_site(predicted.reshape(1, -1), ref.reshape(1, -1))[0])
         passed = sample <= self.tolerance
-        source = "surrogate"
-        if not passed:
-            t_all, _, _ = plain_targets(config, raw_dev, pts, device=dev, plan=plan)
-            psfs = targets_to_planes(t_all)
+        if passed:
+            xp, xc, _ = site_inputs(raw_dev, off, scale=self.model.input_scale, device=dev)
+            psfs = self.model.predict(xp, xc)
+            source = "surrogate"
+        else:
+            psfs = torch.empty((len(pts), PLANES, GRID, GRID), dtype=torch.float32, device=dev)
+            psfs[torch.as_tensor(gate, device=dev)] = ref
+            rest = np.setdiff1d(np.arange(len(pts)), gate)
+            if len(rest):
+                t_rest, _, _ = plain_targets(config, raw_dev, pts[rest], device=dev, plan=plan)
+                psfs[torch.as_tensor(rest, device=dev)] = targets_to_planes(t_rest)
             source = "plain"
         torch.cuda.synchronize(dev)
         return {"psfs": psfs, "source": source, "seconds": time.perf_counter() - t0,

@@ -229,3 +229,9 @@ def test_surrogate_stage_gate():
     assert loose["gate"]["passed"] and loose["source"] == "surrogate"
     np.testing.assert_array_equal(loose["gate"]["sites"], strict["gate"]["sites"])
     assert abs(loose["gate"]["rel_l2"] - strict["gate"]["rel_l2"]) < 1e-9
+    # the gate predicts its own sites first; the full prediction of a passed
+    # gate reproduces the gate's sample error on those sites
+    g = torch.as_tensor(loose["gate"]["sites"], device="cuda")
+    ref_g = S.targets_to_planes(plain)[g]
+    full = float(S.rel_l2_per_site(loose["psfs"][g].reshape(1, -1), ref_g.reshape(1, -1))[0])
+    assert abs(full - loose["gate"]["rel_l2"]) < 1e-6 * max(1.0, full)
