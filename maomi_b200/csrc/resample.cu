@@ -97,7 +97,7 @@ constexpr int kFocalRows = 8;
 
 __global__ void focal_transpose_kernel(const float* __restrict__ focal, const float* __restrict__ axial, float scale,
                                        int Z, int X, int Y, float* __restrict__ psf, double* __restrict__ energies) {
-  extern __shared__ float tile[];  // (rows * Y) x (Z + 1)
+  extern __shared__ __align__(16) float tile[];  // (rows * Y) x Z: the block's output run, in order
   __shared__ double red[32];
   const int p = blockIdx.y, x0 = blockIdx.x * kFocalRows;
   const int rows = min(kFocalRows, X - x0);
@@ -118,18 +118,24 @@ __global__ void focal_transpose_kernel(const float* __restrict__ focal, const fl
       for (int u = 0; u < kFocalBatch; ++u) {
         if (z0 + u >= Z) break;
         const float w = scale * v[u] * __ldg(axial + z0 + u);
-        tile[o * (Z + 1) + z0 + u] = w;
+        tile[o * Z + z0 + u] = w;
         acc += w;
       }
     }
   }
   __syncthreads();
   if (psf) {
-    // one warp per output run of Z values (z fastest): contiguous stores
+    // the tile is the block's whole output run (pixels x planes, z fastest):
+    // a linear copy, 16 bytes per thread and step when aligned
     float* dst = psf + ((size_t)p * X + x0) * Y * Z;
-    const int lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
-    for (int o = warp; o < ry; o += nw)
-      for (int z = lane; z < Z; z += 32) dst[(size_t)o * Z + z] = tile[o * (Z + 1) + z];
+    const int total = ry * Z;
+    if ((total & 3) == 0 && (reinterpret_cast<uintptr_t>(dst) & 15) == 0) {
+      const float4* t4 = reinterpret_cast<const float4*>(tile);
+      float4* d4 = reinterpret_cast<float4*>(dst);
+      for (int i = tid; i < (total >> 2); i += nt) d4[i] = t4[i];
+    } else {
+      for (int i = tid; i < total; i += nt) dst[i] = tile[i];
+    }
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
@@ -149,7 +155,18 @@ __global__ void site_sums_kernel(const float* __restrict__ psf, long long E, int
   if (e >= E) return;
   const int p0 = blockIdx.y * chunk, p1 = min(P, p0 + chunk);
   double s = 0.0, a = 0.0;
-  for (int p = p0; p < p1; ++p) {
+  int p = p0;
+  for (; p + 8 <= p1; p += 8) {  // eight independent loads in flight
+    float v[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) v[u] = __ldg(psf + (size_t)(p + u) * E + e);
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      s += (double)v[u];
+      a += fabs((double)v[u]);
+    }
+  }
+  for (; p < p1; ++p) {
     const double v = __ldg(psf + (size_t)p * E + e);
     s += v;
     a += fabs(v);
@@ -245,7 +262,7 @@ extern "C" int mm_focal_finalize(const float* focal, const int32_t* ix, const fl
   if (identity) {
     MM_CHECK_ARG(X == H && Y == W, "identity focal resample needs X == H and Y == W (got %d x %d from %d x %d)", X, Y,
                  H, W);
-    const size_t tt = sizeof(float) * (size_t)kFocalRows * Y * (Z + 1);
+    const size_t tt = sizeof(float) * (size_t)kFocalRows * Y * Z;
     MM_CHECK_ARG(tt <= 200 * 1024, "focal crop %d x %d planes too large for one tile", Y, Z);
     if (tt > 48 * 1024)
       MM_CHECK_CUDA(cudaFuncSetAttribute(focal_transpose_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tt),
@@ -269,7 +286,7 @@ extern "C" int mm_focal_finalize(const float* focal, const int32_t* ix, const fl
     const long long E = (long long)X * Y * Z;
     MM_CHECK_CUDA(cudaMemsetAsync(psf_sum, 0, sizeof(double) * E, s), "zero psf sum");
     MM_CHECK_CUDA(cudaMemsetAsync(psf_abs_sum, 0, sizeof(double) * E, s), "zero psf abs sum");
-    const int chunk = 64;
+    const int chunk = 128;
     dim3 grid((unsigned)((E + 255) / 256), (unsigned)((P + chunk - 1) / chunk));
     site_sums_kernel<<<grid, 256, 0, s>>>(psf, E, P, chunk, psf_sum, psf_abs_sum);
     MM_CHECK_LAUNCH("site sums");
