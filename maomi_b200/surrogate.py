@@ -8,7 +8,7 @@ BF16 tcgen05 GEMMs (FP32 accumulation) and CUDA-core kernels for the
 spectral mixing, activations, loss and Adam; PyTorch only provides device
 memory, streams and indexing.
 
-The plain propagator is both the teacher and the judge: ``training_set``
+The plain propagator is both the teacher and the gatekeeper: ``training_set``
 builds (inputs, PSF) pairs with it, and ``SurrogateStage.run`` re-propagates a
 seeded fraction of the sites with it and replaces the whole surrogate output
 by the plain result when the sample's relative L2 error exceeds the

@@ -210,7 +210,7 @@ def test_surrogate_training_gains_over_mean_psf():
 
 @pytest.mark.gpu
 def test_surrogate_stage_gate():
-    """The plain propagator judges a seeded 5 % of the sites: a sample error
+    """The plain propagator checks a seeded 5 % of the sites: a sample error
     above the tolerance replaces the whole output by the plain PSFs; below it
     the surrogate output stands."""
     import torch
