@@ -68,8 +68,16 @@ struct ISmem {
   static constexpr size_t bytes = (xbuf + xbuf % 2) * sizeof(float2) + L::kTwiddleBytes + screen * sizeof(float);
 };
 
+// 128-thread CTAs resident per SM the item kernels are compiled for: the
+// 512 window's lines hold 32 samples per thread, which fit 168 registers
+// without spilling at three CTAs per SM (the line default is two).
+template <class L>
+constexpr int items_min_blocks() {
+  return L::N == 512 ? 3 : L::kMinBlocks;
+}
+
 template <class L, int LINES>
-__global__ void __launch_bounds__(LINES * L::R2, L::kMinBlocks * 128 / (LINES * L::R2)) items_kernel(ItemP p) {
+__global__ void __launch_bounds__(LINES * L::R2, items_min_blocks<L>() * 128 / (LINES * L::R2)) items_kernel(ItemP p) {
   constexpr int R1 = L::R1, R2 = L::R2, N = L::N;
   extern __shared__ float4 smem_raw[];
   float2* xa = reinterpret_cast<float2*>(smem_raw);
