@@ -17,17 +17,18 @@ import numpy as np
 from . import _lib
 
 MIN_SIZE, MAX_SIZE = 64, 1024
+# transform sizes of one axis: 768 = 48 x 16 lines serve FP32 planes (a
+# float64 spectrum asked for 768 runs at 1024, see KernelSpectrum)
+SIZES = (64, 128, 256, 512, 768, 1024)
 
 
 def transform_size(need):
-    """Smallest supported power of two >= ``need``."""
-    n = MIN_SIZE
-    while n < need:
-        n *= 2
-    if n > MAX_SIZE:
-        raise ValueError(f"plane convolution needs a transform of {need} samples; this build supports up to "
-                         f"{MAX_SIZE} (volumes up to about {MAX_SIZE} pixels across with small kernels)")
-    return n
+    """Smallest supported transform size >= ``need``."""
+    for n in SIZES:
+        if n >= need:
+            return n
+    raise ValueError(f"plane convolution needs a transform of {need} samples; this build supports up to "
+                     f"{MAX_SIZE} (volumes up to about {MAX_SIZE} pixels across with small kernels)")
 
 
 def real_dtype(t):
@@ -57,7 +58,10 @@ class KernelSpectrum:
     """Device half spectra of (grouped) kernel planes at one transform size.
 
     ``fx``, ``fy``: transform sizes; ``kx``, ``ky``: kernel plane extents;
-    ``planes``: kernel transform planes (after grouping); ``fp64``."""
+    ``planes``: kernel transform planes (after grouping); ``fp64``.  A
+    float64 kernel asked for a 768-point axis gets 1024 (the 48-point line
+    transform is FP32 only); any size at least the one asked for is alias-free.
+    Every convolution and spectrum buffer takes its sizes from ``desc``."""
 
     def __init__(self, kernel, fx, fy, *, group=1):
         import torch
@@ -65,6 +69,8 @@ class KernelSpectrum:
         self.fp64 = real_dtype(kernel)
         self.dtype = kernel.dtype
         self.fx, self.fy = int(fx), int(fy)
+        if self.fp64:
+            self.fx, self.fy = (1024 if f == 768 else f for f in (self.fx, self.fy))
         self.kx, self.ky = int(kernel.shape[0]), int(kernel.shape[1])
         self.group = int(group)
         self.planes = -(-int(kernel.shape[2]) // self.group)

@@ -44,6 +44,7 @@ template <> struct Split<64> { static constexpr int R1 = 8, R2 = 8; };
 template <> struct Split<128> { static constexpr int R1 = 16, R2 = 8; };
 template <> struct Split<256> { static constexpr int R1 = 16, R2 = 16; };
 template <> struct Split<512> { static constexpr int R1 = 32, R2 = 16; };
+template <> struct Split<768> { static constexpr int R1 = 48, R2 = 16; };  // FP32 planes only
 template <> struct Split<1024> { static constexpr int R1 = 32, R2 = 32; };
 
 constexpr int kThreads = 256;
@@ -65,6 +66,43 @@ __host__ __device__ constexpr int slot(int m) {
   return (m % (R1 / R2)) * R2 + m / (R1 / R2);
 }
 
+// 48-point DFT in registers, natural order in and out: n = 3 m + r, k = k1 +
+// 16 k2; three 16-point DFTs over m, twiddles W_48^(r k1) (entry stride * r *
+// k1 of the line's table of W_N^n, conjugated for SIGN > 0), then radix-3
+// butterflies over r: X[k1 + 16 k2] = sum_r W_3^(r k2) W_48^(r k1) F_r[k1].
+template <int SIGN, class C>
+__device__ __forceinline__ void dft48(C (&v)[48], const C* tw, int stride) {
+  using R = decltype(v[0].x);
+  C f[3][16];
+#pragma unroll
+  for (int r = 0; r < 3; ++r) {
+#pragma unroll
+    for (int m = 0; m < 16; ++m) f[r][m] = v[3 * m + r];
+    dft<16, SIGN>(f[r]);
+  }
+#pragma unroll
+  for (int r = 1; r < 3; ++r)
+#pragma unroll
+    for (int k1 = 1; k1 < 16; ++k1) {
+      C w = tw[stride * r * k1];
+      if constexpr (SIGN > 0) w.y = -w.y;
+      f[r][k1] = cmul(f[r][k1], w);
+    }
+  const R h = R(0.5), q = R(SIGN) * R(0.86602540378443864676);  // SIGN * sqrt(3) / 2
+#pragma unroll
+  for (int k1 = 0; k1 < 16; ++k1) {
+    const C a = f[0][k1], t1 = cadd(f[1][k1], f[2][k1]), t2 = csub(f[1][k1], f[2][k1]);
+    C m1 = a, m2 = t2;
+    m1.x = a.x - h * t1.x;
+    m1.y = a.y - h * t1.y;
+    m2.x = -q * t2.y;  // i * SIGN * sqrt(3)/2 * (b - c)
+    m2.y = q * t2.x;
+    v[k1] = cadd(a, t1);
+    v[k1 + 16] = cadd(m1, m2);
+    v[k1 + 32] = csub(m1, m2);
+  }
+}
+
 // In-place DFT of one line (SIGN -1 forward, +1 inverse, unnormalised).
 // Thread t holds x[t + R2*m] in v[m]; on return it holds X[t + R2*m] in
 // v[slot(m)].  xb: R1 * (R2 + 1) complex of this line.  Every thread of the
@@ -72,7 +110,10 @@ __host__ __device__ constexpr int slot(int m) {
 template <int R1, int R2, int SIGN, class C>
 __device__ __forceinline__ void line_dft(C (&v)[R1], int t, C* xb, const C* tw) {
   constexpr int J = R1 / R2, P = R2 + 1;
-  dft<R1, SIGN>(v);
+  if constexpr (R1 == 48)
+    dft48<SIGN>(v, tw, R2);  // W_48^j = W_N^(j * N / 48), N / 48 = R2
+  else
+    dft<R1, SIGN>(v);
 #pragma unroll
   for (int k1 = 1; k1 < R1; ++k1) {
     C w = tw[t * k1];
@@ -138,7 +179,7 @@ struct RowShape {
 
 // Forward row pass.  grid (ext_x, ceil(pairs / LPC)); S: (pairs, fx, N).
 template <class T, int N>
-__global__ void __launch_bounds__(kThreads) rows_fwd_kernel(Planes P, int fx, typename Cplx<T>::type* __restrict__ S,
+__global__ void __launch_bounds__(kThreads, N == 768 ? 2 : 1) rows_fwd_kernel(Planes P, int fx, typename Cplx<T>::type* __restrict__ S,
                                                             int pairs) {
   using Sh = RowShape<T, N>;
   using C = typename Sh::C;
@@ -197,7 +238,7 @@ struct ColShape {
 };
 
 template <class T, int N, int SIGN>
-__global__ void __launch_bounds__(kThreads) cols_kernel(typename Cplx<T>::type* __restrict__ S, int fy, int rows_in,
+__global__ void __launch_bounds__(kThreads, N == 768 ? 2 : 1) cols_kernel(typename Cplx<T>::type* __restrict__ S, int fy, int rows_in,
                                                         int row0, int rows_out) {
   using Sh = ColShape<T, N>;
   using C = typename Sh::C;
@@ -292,7 +333,7 @@ __global__ void __launch_bounds__(kCombineThreads) combine_kernel(const typename
   if (b >= nb) return;  // no barriers below
   const int kx = int(b / hy), ky = int(b - (long long)kx * hy);
   if ((ky == 0 || ky == fy / 2) && kx > fx / 2) return;  // its partner handles the pair
-  const int mx = (fx - kx) & (fx - 1), my = (fy - ky) & (fy - 1);
+  const int mx = kx == 0 ? 0 : fx - kx, my = ky == 0 ? 0 : fy - ky;  // conjugate bin
   const bool self = (mx == kx) && (my == ky);
   const long long plane = (long long)fx * fy;
   const long long ik = (long long)kx * fy + ky, im = (long long)mx * fy + my;
@@ -397,7 +438,7 @@ __global__ void unpack_kernel(const typename Cplx<T>::type* __restrict__ S, type
     const int p = int(e / nb);
     const long long b = e - (long long)p * nb;
     const int kx = int(b / hy), ky = int(b - (long long)kx * hy);
-    const int mx = (fx - kx) & (fx - 1), my = (fy - ky) & (fy - 1);
+    const int mx = kx == 0 ? 0 : fx - kx, my = ky == 0 ? 0 : fy - ky;  // conjugate bin
     C a, bb;
     hsplit(S[p * plane + (long long)kx * fy + ky], S[p * plane + (long long)mx * fy + my], a, bb);
     K[(2 * p) * nb + b] = a;
@@ -417,7 +458,7 @@ struct Out {
 };
 
 template <class T, int N>
-__global__ void __launch_bounds__(kThreads) rows_inv_kernel(const typename Cplx<T>::type* __restrict__ S, int fx,
+__global__ void __launch_bounds__(kThreads, N == 768 ? 2 : 1) rows_inv_kernel(const typename Cplx<T>::type* __restrict__ S, int fx,
                                                             Out O) {
   using Sh = RowShape<T, N>;
   using C = typename Sh::C;
@@ -497,15 +538,10 @@ __global__ void background_kernel(BgVols<T> V, int nvol, long long s0, long long
 }
 
 // ------------------------------------------------------------------- host
-int log2_size(int n) {
-  switch (n) {
-    case 64: return 6;
-    case 128: return 7;
-    case 256: return 8;
-    case 512: return 9;
-    case 1024: return 10;
-    default: return -1;
-  }
+// Transform sizes of one axis: powers of two 64..1024, and 768 = 48 x 16 for
+// FP32 planes.
+bool supported_size(int n, int fp64) {
+  return n == 64 || n == 128 || n == 256 || n == 512 || n == 1024 || (n == 768 && !fp64);
 }
 
 template <class T>
@@ -559,9 +595,13 @@ int by_size(int n, F&& f) {
     case 128: return f(std::integral_constant<int, 128>{});
     case 256: return f(std::integral_constant<int, 256>{});
     case 512: return f(std::integral_constant<int, 512>{});
+    case 768:
+      if constexpr (std::is_same_v<T, float>) return f(std::integral_constant<int, 768>{});
+      set_error("scan transform size 768 is for FP32 planes only");
+      return MM_ERR_UNSUPPORTED;
     case 1024: return f(std::integral_constant<int, 1024>{});
     default:
-      set_error("scan transform size %d is not a power of two in 64..1024", n);
+      set_error("scan transform size %d is not one of 64, 128, 256, 512, 768 (FP32), 1024", n);
       return MM_ERR_UNSUPPORTED;
   }
 }
@@ -569,8 +609,8 @@ int by_size(int n, F&& f) {
 int check_desc(const mm_scan_desc* d) {
   MM_CHECK_ARG(d != nullptr, "scan: null descriptor");
   MM_CHECK_ARG(d->fp64 == 0 || d->fp64 == 1, "scan: fp64 must be 0 or 1");
-  if (log2_size(d->fx) < 0 || log2_size(d->fy) < 0) {
-    set_error("scan transform sizes %d x %d: each must be a power of two in 64..1024", d->fx, d->fy);
+  if (!supported_size(d->fx, d->fp64) || !supported_size(d->fy, d->fp64)) {
+    set_error("scan transform sizes %d x %d: each must be 64, 128, 256, 512, 1024 or (FP32) 768", d->fx, d->fy);
     return MM_ERR_UNSUPPORTED;
   }
   MM_CHECK_ARG(d->kx >= 1 && d->ky >= 1 && d->kplanes >= 1, "scan: kernel extents must be positive");

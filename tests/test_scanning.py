@@ -67,7 +67,8 @@ def test_transform_sizes():
     assert transform_size(1) == 64
     assert transform_size(64) == 64
     assert transform_size(65) == 128
-    assert transform_size(532) == 1024
+    assert transform_size(532) == 768  # 48 x 16 lines (FP32 planes)
+    assert transform_size(769) == 1024
     with pytest.raises(ValueError):
         transform_size(1025)
 
@@ -108,7 +109,9 @@ def test_zstack_gpu_even_kernel_contract():
 @pytest.mark.gpu
 def test_zstack_gpu_benchmark_size():
     """The static scan of run_fixed at the benchmark size: 512 x 512 x 60
-    volume, the 40 x 40 x 46 stage PSF, both masks (FP32 like run_fixed)."""
+    volume, the 40 x 40 x 46 stage PSF, both masks (FP32 like run_fixed).
+    Both modes run on 768-point lines in FP32 (transforms of 532 and 551
+    samples); FP64 planes take 1024-point lines for the same request."""
     from maomi_b200.scanning import zstack
     rng = np.random.default_rng(11)
     v = rng.uniform(0, 1, (512, 512, 60)).astype(np.float32)
@@ -117,6 +120,11 @@ def test_zstack_gpu_benchmark_size():
     m2 = rng.uniform(0.2, 1.0, (512, 512)).astype(np.float32)
     got = zstack(v, p, mask=m1, collection_mask=m2, device="cuda").cpu().numpy()
     assert rel_l2(got, S.zstack(v, p, mask=m1, collection_mask=m2)) < FP32_TOL
+    got = zstack(v, p, mode="legacy_circular", device="cuda").cpu().numpy()
+    assert rel_l2(got, S.zstack(v, p, mode="legacy_circular")) < FP32_TOL
+    v64, p64 = v[:, :, :8].astype(np.float64), p[:, :, :6].astype(np.float64)
+    got = zstack(v64, p64, device="cuda").cpu().numpy()
+    assert got.dtype == np.float64 and rel_l2(got, S.zstack(v64, p64)) < FP64_TOL
 
 
 @pytest.mark.gpu
