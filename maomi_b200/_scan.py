@@ -17,9 +17,10 @@ import numpy as np
 from . import _lib
 
 MIN_SIZE, MAX_SIZE = 64, 1024
-# transform sizes of one axis: 768 = 48 x 16 lines serve FP32 planes (a
-# float64 spectrum asked for 768 runs at 1024, see KernelSpectrum)
-SIZES = (64, 128, 256, 512, 768, 1024)
+# transform sizes of one axis: 384 = 48 x 8 and 768 = 48 x 16 lines serve
+# FP32 planes (a float64 spectrum asked for them runs at 512 / 1024, see
+# KernelSpectrum)
+SIZES = (64, 128, 256, 384, 512, 768, 1024)
 
 
 def transform_size(need):
@@ -59,8 +60,9 @@ class KernelSpectrum:
 
     ``fx``, ``fy``: transform sizes; ``kx``, ``ky``: kernel plane extents;
     ``planes``: kernel transform planes (after grouping); ``fp64``.  A
-    float64 kernel asked for a 768-point axis gets 1024 (the 48-point line
-    transform is FP32 only); any size at least the one asked for is alias-free.
+    float64 kernel asked for a 384- or 768-point axis gets 512 or 1024 (the
+    48-point line transform is FP32 only); any size at least the one asked for
+    is alias-free.
     Every convolution and spectrum buffer takes its sizes from ``desc``."""
 
     def __init__(self, kernel, fx, fy, *, group=1):
@@ -70,7 +72,7 @@ class KernelSpectrum:
         self.dtype = kernel.dtype
         self.fx, self.fy = int(fx), int(fy)
         if self.fp64:
-            self.fx, self.fy = (1024 if f == 768 else f for f in (self.fx, self.fy))
+            self.fx, self.fy = ({384: 512, 768: 1024}.get(f, f) for f in (self.fx, self.fy))
         self.kx, self.ky = int(kernel.shape[0]), int(kernel.shape[1])
         self.group = int(group)
         self.planes = -(-int(kernel.shape[2]) // self.group)

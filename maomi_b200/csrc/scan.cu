@@ -44,6 +44,7 @@ template <> struct Split<64> { static constexpr int R1 = 8, R2 = 8; };
 template <> struct Split<128> { static constexpr int R1 = 16, R2 = 8; };
 template <> struct Split<256> { static constexpr int R1 = 16, R2 = 16; };
 template <> struct Split<512> { static constexpr int R1 = 32, R2 = 16; };
+template <> struct Split<384> { static constexpr int R1 = 48, R2 = 8; };   // FP32 planes only
 template <> struct Split<768> { static constexpr int R1 = 48, R2 = 16; };  // FP32 planes only
 template <> struct Split<1024> { static constexpr int R1 = 32, R2 = 32; };
 
@@ -179,7 +180,7 @@ struct RowShape {
 
 // Forward row pass.  grid (ext_x, ceil(pairs / LPC)); S: (pairs, fx, N).
 template <class T, int N>
-__global__ void __launch_bounds__(kThreads, N == 768 ? 2 : 1) rows_fwd_kernel(Planes P, int fx, typename Cplx<T>::type* __restrict__ S,
+__global__ void __launch_bounds__(kThreads, Split<N>::R1 == 48 ? 2 : 1) rows_fwd_kernel(Planes P, int fx, typename Cplx<T>::type* __restrict__ S,
                                                             int pairs) {
   using Sh = RowShape<T, N>;
   using C = typename Sh::C;
@@ -238,7 +239,7 @@ struct ColShape {
 };
 
 template <class T, int N, int SIGN>
-__global__ void __launch_bounds__(kThreads, N == 768 ? 2 : 1) cols_kernel(typename Cplx<T>::type* __restrict__ S, int fy, int rows_in,
+__global__ void __launch_bounds__(kThreads, Split<N>::R1 == 48 ? 2 : 1) cols_kernel(typename Cplx<T>::type* __restrict__ S, int fy, int rows_in,
                                                         int row0, int rows_out) {
   using Sh = ColShape<T, N>;
   using C = typename Sh::C;
@@ -458,7 +459,7 @@ struct Out {
 };
 
 template <class T, int N>
-__global__ void __launch_bounds__(kThreads, N == 768 ? 2 : 1) rows_inv_kernel(const typename Cplx<T>::type* __restrict__ S, int fx,
+__global__ void __launch_bounds__(kThreads, Split<N>::R1 == 48 ? 2 : 1) rows_inv_kernel(const typename Cplx<T>::type* __restrict__ S, int fx,
                                                             Out O) {
   using Sh = RowShape<T, N>;
   using C = typename Sh::C;
@@ -538,10 +539,10 @@ __global__ void background_kernel(BgVols<T> V, int nvol, long long s0, long long
 }
 
 // ------------------------------------------------------------------- host
-// Transform sizes of one axis: powers of two 64..1024, and 768 = 48 x 16 for
-// FP32 planes.
+// Transform sizes of one axis: powers of two 64..1024, and 384 = 48 x 8 and
+// 768 = 48 x 16 for FP32 planes.
 bool supported_size(int n, int fp64) {
-  return n == 64 || n == 128 || n == 256 || n == 512 || n == 1024 || (n == 768 && !fp64);
+  return n == 64 || n == 128 || n == 256 || n == 512 || n == 1024 || ((n == 384 || n == 768) && !fp64);
 }
 
 template <class T>
@@ -594,6 +595,10 @@ int by_size(int n, F&& f) {
     case 64: return f(std::integral_constant<int, 64>{});
     case 128: return f(std::integral_constant<int, 128>{});
     case 256: return f(std::integral_constant<int, 256>{});
+    case 384:
+      if constexpr (std::is_same_v<T, float>) return f(std::integral_constant<int, 384>{});
+      set_error("scan transform size 384 is for FP32 planes only");
+      return MM_ERR_UNSUPPORTED;
     case 512: return f(std::integral_constant<int, 512>{});
     case 768:
       if constexpr (std::is_same_v<T, float>) return f(std::integral_constant<int, 768>{});
@@ -601,7 +606,7 @@ int by_size(int n, F&& f) {
       return MM_ERR_UNSUPPORTED;
     case 1024: return f(std::integral_constant<int, 1024>{});
     default:
-      set_error("scan transform size %d is not one of 64, 128, 256, 512, 768 (FP32), 1024", n);
+      set_error("scan transform size %d is not one of 64, 128, 256, 384 (FP32), 512, 768 (FP32), 1024", n);
       return MM_ERR_UNSUPPORTED;
   }
 }
@@ -610,7 +615,8 @@ int check_desc(const mm_scan_desc* d) {
   MM_CHECK_ARG(d != nullptr, "scan: null descriptor");
   MM_CHECK_ARG(d->fp64 == 0 || d->fp64 == 1, "scan: fp64 must be 0 or 1");
   if (!supported_size(d->fx, d->fp64) || !supported_size(d->fy, d->fp64)) {
-    set_error("scan transform sizes %d x %d: each must be 64, 128, 256, 512, 1024 or (FP32) 768", d->fx, d->fy);
+    set_error("scan transform sizes %d x %d: each must be 64, 128, 256, 512, 1024 or (FP32) 384, 768", d->fx,
+              d->fy);
     return MM_ERR_UNSUPPORTED;
   }
   MM_CHECK_ARG(d->kx >= 1 && d->ky >= 1 && d->kplanes >= 1, "scan: kernel extents must be positive");

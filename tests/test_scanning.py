@@ -67,6 +67,7 @@ def test_transform_sizes():
     assert transform_size(1) == 64
     assert transform_size(64) == 64
     assert transform_size(65) == 128
+    assert transform_size(257) == 384  # 48 x 8 lines (FP32 planes)
     assert transform_size(532) == 768  # 48 x 16 lines (FP32 planes)
     assert transform_size(769) == 1024
     with pytest.raises(ValueError):
@@ -163,6 +164,27 @@ def test_blurred_background_gpu(name, idx):
     got = blurred_background(d["b_volume"], idx, spec, frequency=True, **kw)
     assert rel_l2(got, ref) < FP32_TOL
     assert rel_l2(got, d[f"b_{name}_freq"]) < FP32_TOL
+
+
+@pytest.mark.gpu
+def test_zstack_gpu_384_point_lines():
+    """A 300 x 330 x 12 FP32 volume with a 21 x 9 x 5 PSF needs transforms of
+    310 x 334 samples (MATLAB crop) or 320 x 338 (periodic mode): 384 = 48 x 8
+    lines in both directions (FP32); the FP64 volume takes 512-point lines
+    for the same request."""
+    from maomi_b200._scan import transform_size
+    from maomi_b200.scanning import zstack
+    assert transform_size(320) == 384 and transform_size(338) == 384
+    rng = np.random.default_rng(12)
+    v = rng.uniform(0, 1, (300, 330, 12)).astype(np.float32)
+    p = rng.uniform(0, 1, (21, 9, 5)).astype(np.float32)
+    m1 = rng.uniform(0.5, 1.5, (300, 330)).astype(np.float32)
+    got = zstack(v, p, mask=m1, device="cuda").cpu().numpy()
+    assert rel_l2(got, S.zstack(v, p, mask=m1)) < FP32_TOL
+    got = zstack(v, p, mode="legacy_circular", device="cuda").cpu().numpy()
+    assert rel_l2(got, S.zstack(v, p, mode="legacy_circular")) < FP32_TOL
+    v64, p64 = v.astype(np.float64), p.astype(np.float64)
+    assert rel_l2(zstack(v64, p64, device="cuda").cpu().numpy(), S.zstack(v64, p64)) < FP64_TOL
 
 
 @pytest.mark.gpu
