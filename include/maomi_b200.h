@@ -519,7 +519,8 @@ int mm_surrogate_planes(const float* y, float* out, int sites, void* stream);
 /* ------------------------------------------------------------------------
  * Static and per-frame scan operators: 2-D linear convolutions of real
  * planes with real kernel planes through zero-padded 2-D DFTs (sizes
- * fx x fy, powers of two 64..1024) and a per-bin coupling rule along Z.
+ * fx x fy: 64, 128, 256, 512, 1024, and for FP32 planes 384 and 768) and a
+ * per-bin coupling rule along Z.
  *
  * Replaces:
  *   zstack                 maomi/scanning.py:8-53   (CONV_Z / CORR_Z rules)
@@ -552,7 +553,7 @@ typedef struct {
 
 typedef struct {
   int fp64;               /* 0: float32 data / FP32 transforms; 1: float64 / FP64 */
-  int fx, fy;             /* transform sizes: powers of two in 64..1024 */
+  int fx, fy;             /* transform sizes: 64, 128, 256, 512, 1024; 384, 768 with fp64 = 0 */
   int kx, ky;             /* kernel plane extents */
   int kplanes;            /* kernel transform planes (after grouping) */
 } mm_scan_desc;
